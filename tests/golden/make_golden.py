@@ -1,0 +1,245 @@
+"""Generate golden fixtures by running the reference solver itself.
+
+Run in a container that has the reference source tree (read-only):
+
+    python tests/golden/make_golden.py --ref /root/reference [--skip-arm]
+
+The reference (NinhGhoster/TO-F450-arm, pure Python + SciPy) is imported from
+its own `src/` and `sims/` packages and driven with the synthetic geometries of
+`tof_b200.geometry` / `tof_b200.configs` (inputs only).  Two solver branches of
+the reference are made exact for the fixtures:
+
+* static solves call `FEM3D.apply_BCs_and_solve(..., method="lu")`, the
+  reference's own direct branch (src/fem.py:551-552);
+* `scipy.sparse.linalg.lobpcg` as seen by src/fem.py is replaced by a tight
+  shift-invert `eigsh` (sigma = 0, tol 1e-13) on the same K_ff / M_ff, because
+  the reference's LOBPCG at tol 1e-4 is not an accuracy oracle (it misses f1
+  by up to 16 % on the production domain).  Everything else in
+  `modal_analysis` (assembly, tip mass, sorting, clamping, padding) is the
+  reference's code.
+
+Fixtures are written next to this script.  Nothing on the GPU test path reads
+the reference; only these .npz files travel.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+import scipy.sparse.linalg as spla
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "to-f450-arm_b200"))
+
+from tof_b200 import configs as C  # noqa: E402
+from tof_b200.geometry import BoxGeometry  # noqa: E402
+
+
+def exact_eigs(K, X, B=None, M=None, tol=None, largest=False, maxiter=None, **kw):
+    k = X.shape[1]
+    lam, V = spla.eigsh(K.tocsc(), k=k, M=B.tocsc(), sigma=0.0, which="LM", tol=1e-13,
+                        maxiter=50000)
+    return lam, V
+
+
+def sign_fix(modes):
+    """Make the largest-magnitude entry of each mode positive."""
+    out = modes.copy()
+    for k in range(out.shape[1]):
+        i = np.argmax(np.abs(out[:, k]))
+        if out[i, k] < 0:
+            out[:, k] *= -1
+    return out
+
+
+def setup_reference(ref):
+    sys.path.insert(0, ref)
+    import src.fem as rfem
+    import src.topopt as rtop
+    rfem.spla.lobpcg = exact_eigs          # exact eigenpairs, see module docstring
+    from sims import modal_participation as rmp
+    return rfem, rtop, rmp
+
+
+def mat_ref(rfem):
+    return rfem.Material(E=C.PA12.E, nu=C.PA12.nu, sigma_y=C.PA12.sigma_y,
+                         sigma_u=C.PA12.sigma_u, rho=C.PA12.rho)
+
+
+def geom_arrays(geom, fem):
+    m = geom.build_masks()
+    return dict(nx=geom.nx, ny=geom.ny, nz=geom.nz, h=np.array([geom.dx, geom.dy, geom.dz]),
+                in_arm=m["in_arm"], design=m["design"], keep_solid=m["keep_solid"],
+                fixed_dofs=fem.fixed_dofs, free_dofs=fem.free_dofs,
+                tip_nodes=geom.motor_mount_top_nodes(),
+                Ke=fem.Ke_solid, Me=fem.Me_solid)
+
+
+def tiny_geometry():
+    nx, ny, nz = 6, 3, 3
+    in_arm = np.ones((nx, ny, nz), bool)
+    in_arm[5, 2, 2] = False            # corner voxel removed -> node (6,3,3) is a ghost
+    in_arm[2, 1, 1] = False            # interior hole
+    keep = np.zeros_like(in_arm)
+    keep[0, :, :] = True
+    g = BoxGeometry(nx, ny, nz, 2e-3, 2e-3, 2e-3, clamp="root_face", mount="tip_face",
+                    in_arm_mask=in_arm, keep_solid_mask=keep)
+    return g
+
+
+def make_tiny(rfem, rtop, rmp):
+    g = tiny_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    rng = np.random.default_rng(1)
+    rho = rng.uniform(0.03, 1.0, fem.n_active)
+    rho[:3] = [0.05, 0.1, 0.0999]            # both branches of the mass penalty
+    F1 = g.load_vector(F=(0.0, 0.0, -5.0))
+    F2 = g.load_vector(F=(0.0, 3.0, 1.0), Mz=0.05)
+    K = fem.assemble_K(rho)
+    M = fem.assemble_M(rho, tip_mass_kg=0.06, tip_mass_nodes=g.motor_mount_top_nodes())
+    fr = fem.free_dofs
+    X = np.zeros((g.n_dofs, 3))
+    X[fr] = rng.standard_normal((len(fr), 3))
+    KX = np.zeros_like(X)
+    MX = np.zeros_like(X)
+    KX[fr] = K[fr][:, fr] @ X[fr]
+    MX[fr] = M[fr][:, fr] @ X[fr]
+    u1 = fem.apply_BCs_and_solve(K, F1, method="lu")
+    u2 = fem.apply_BCs_and_solve(K, F2, method="lu")
+    ce1 = fem.elem_compliance(u1, rho)
+    freqs, modes, lam = fem.modal_analysis(rho, n_modes=4, tip_mass_kg=0.06)
+    dlam0 = fem.eigenvalue_sensitivity(rho, lam[0], modes[:, 0], tip_mass_kg=0.06)
+    eff = rmp.effective_mass_voxel(fem, g, rho, modes, 0.06, direction=2)
+    masks = g.build_masks()
+    field = rng.standard_normal((g.nx, g.ny, g.nz))
+    k15 = rtop.cone_kernel(1.5)
+    k23 = rtop.cone_kernel(2.3)
+    filt15 = rtop.filter_field(field, masks["design"], k15)
+    filt23 = rtop.filter_field(field, masks["in_arm"], k23)
+    return dict(geom_arrays(g, fem), rho=rho, F1=F1, F2=F2, X=X, KX=KX, MX=MX,
+                diagK=K.diagonal(), diagM=M.diagonal(),
+                u1=u1, u2=u2, ce1=ce1, freqs=freqs, lam=lam, modes=sign_fix(modes),
+                dlam0=dlam0, eff=eff, field=field, k15=k15, k23=k23,
+                filt15=filt15, filt23=filt23, total_mass=fem.total_mass(rho),
+                elem_dof_ids=fem.elem_dof_ids)
+
+
+def make_oc(rtop):
+    """The OC update on its own (src/topopt.py:190-214) via a stub optimiser."""
+    rng = np.random.default_rng(2)
+    x = rng.uniform(0.001, 1.0, 500)
+    dc = -rng.uniform(1e-6, 1e-2, 500)
+
+    class Stub:
+        V_e = 8e-9
+        move = 0.2
+        target_volume = 0.3 * 500 * 8e-9
+    x_new = rtop.SIMPOptimizer._oc_update(Stub(), x, dc)
+    return dict(x=x, dc=dc, V_e=Stub.V_e, move=Stub.move, target_volume=Stub.target_volume,
+                x_new=x_new)
+
+
+def simp_geometry():
+    return C.arm_geometry(nx=16, ny=4, nz=4, h=2e-3, mount_cols=2)
+
+
+def make_simp(rfem, rtop):
+    g = simp_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    orig = rfem.FEM3D.apply_BCs_and_solve
+
+    def lu_solve(self, K, F, method="cg", x0=None, rtol=1e-5):
+        return orig(self, K, F, method="lu")
+    rfem.FEM3D.apply_BCs_and_solve = lu_solve
+    try:
+        F = C.arm_static_loads(g)[:2]
+        opt = rtop.SIMPOptimizer(g, fem, load_cases=[dict(F=(0, 0, 0))] * 2,
+                                 weights=[0.6, 0.4], vol_frac=0.3, r_min_mm=3.0, max_iter=4,
+                                 tol_change=0.0, min_freq_Hz=1500.0, tip_mass_kg=0.06,
+                                 n_modes_track=3, mu_freq_init=0.2, mu_freq_ramp_every=2)
+        opt.F_list = [f.copy() for f in F]
+        res = opt.run(verbose=False)
+    finally:
+        rfem.FEM3D.apply_BCs_and_solve = orig
+    h = res["history"]
+    return dict(geom_arrays(g, fem), F1=F[0], F2=F[1], weights=np.array([0.6, 0.4]),
+                vol_frac=0.3, r_min_mm=3.0, min_freq_Hz=1500.0, mu_init=0.2, ramp_every=2,
+                n_iter=4, n_modes=3,
+                compliance=np.array(h["compliance"]), change=np.array(h["change"]),
+                vf_hist=np.array(h["vol_frac"]), omega1=np.array(h["omega_1_Hz"]),
+                mu_hist=np.array(h["mu_freq"]), viol=np.array(h["freq_violation"]),
+                rho_final=res["rho_active"])
+
+
+def make_cantilever(rfem, rmp):
+    g = C.cantilever_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    rho = C.cantilever_density(g)
+    F = C.cantilever_loads(g)[0]
+    K = fem.assemble_K(rho)
+    t = time.time()
+    u = fem.apply_BCs_and_solve(K, F, method="lu")
+    t_lu = time.time() - t
+    t = time.time()
+    u_cg = fem.apply_BCs_and_solve(K, F, method="cg", rtol=1e-8)
+    t_cg = time.time() - t
+    fr = fem.free_dofs
+    Kff = K[fr][:, fr]
+    relres_cg = np.linalg.norm(F[fr] - Kff @ u_cg[fr]) / np.linalg.norm(F[fr])
+    t = time.time()
+    freqs, modes, lam = fem.modal_analysis(rho, n_modes=6, tip_mass_kg=0.0)
+    t_eig = time.time() - t
+    eff = rmp.effective_mass_voxel(fem, g, rho, modes, 0.0, direction=2)
+    ce = fem.elem_compliance(u, rho)
+    dlam0 = fem.eigenvalue_sensitivity(rho, lam[0], modes[:, 0], tip_mass_kg=0.0)
+    print(f"cantilever: lu {t_lu:.2f}s  cg(1e-8) {t_cg:.2f}s relres {relres_cg:.2e}  eig {t_eig:.1f}s")
+    return dict(geom_arrays(g, fem), rho=rho, F=F, u=u, compliance=float(F @ u), ce=ce,
+                freqs=freqs, lam=lam, eff=eff, dlam0=dlam0, relres_cg=relres_cg,
+                t_cg=t_cg)
+
+
+def make_arm(rfem, rmp):
+    g = C.arm_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    rho = C.arm_hollow_density(g)
+    F = C.arm_static_loads(g)[0]
+    K = fem.assemble_K(rho)
+    t = time.time()
+    u = fem.apply_BCs_and_solve(K, F, method="lu")
+    t_lu = time.time() - t
+    t = time.time()
+    freqs, modes, lam = fem.modal_analysis(rho, n_modes=6, tip_mass_kg=C.TIP_MASS_KG)
+    t_eig = time.time() - t
+    eff = rmp.effective_mass_voxel(fem, g, rho, modes, C.TIP_MASS_KG, direction=2)
+    ce = fem.elem_compliance(u, rho)
+    dlam0 = fem.eigenvalue_sensitivity(rho, lam[0], modes[:, 0], tip_mass_kg=C.TIP_MASS_KG)
+    rng = np.random.default_rng(3)
+    sample = np.sort(rng.choice(fem.n_active, 512, replace=False))
+    dof_sample = np.sort(rng.choice(fem.free_dofs, 2048, replace=False))
+    print(f"arm: lu {t_lu:.1f}s  eig {t_eig:.1f}s  freqs {freqs}")
+    return dict(geom_arrays(g, fem), rho=rho, F=F, compliance=float(F @ u),
+                u_sample=u[dof_sample], dof_sample=dof_sample,
+                ce_sample=ce[sample], dlam0_sample=dlam0[sample], elem_sample=sample,
+                freqs=freqs, lam=lam, eff=eff, umax=np.abs(u).max())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--skip-arm", action="store_true")
+    a = ap.parse_args()
+    rfem, rtop, rmp = setup_reference(a.ref)
+    np.savez_compressed(os.path.join(HERE, "tiny.npz"), **make_tiny(rfem, rtop, rmp))
+    np.savez_compressed(os.path.join(HERE, "oc.npz"), **make_oc(rtop))
+    np.savez_compressed(os.path.join(HERE, "simp_small.npz"), **make_simp(rfem, rtop))
+    np.savez_compressed(os.path.join(HERE, "cantilever.npz"), **make_cantilever(rfem, rmp))
+    if not a.skip_arm:
+        np.savez_compressed(os.path.join(HERE, "arm.npz"), **make_arm(rfem, rmp))
+
+
+if __name__ == "__main__":
+    main()
