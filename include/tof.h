@@ -1,0 +1,189 @@
+/* libtof — B200 (sm_100a) voxel SIMP hot path behind a plain C ABI.
+ *
+ * Every entry point takes plain pointers and sizes; device pointers are CUDA
+ * global-memory addresses on the current device, `stream` is a cudaStream_t
+ * passed as void* (NULL = the legacy default stream).  Return value: 0 on
+ * success, > 0 "finished but not converged", < 0 an error (see TOF_ERR_*;
+ * tof_last_error() has the message).  Nothing here falls back to the CPU.
+ *
+ * Vector layout ("node4"): a nodal vector of the (nx+1)(ny+1)(nz+1)-node grid
+ * stores node n = k*(nx+1)*(ny+1) + j*(nx+1) + i at [4n .. 4n+3] as
+ * (ux, uy, uz, 0); a block of R vectors is R such arrays back to back.
+ * tof_pack / tof_unpack convert from / to the reference's DOF-major layout
+ * (DOF 3n + c).  All node4 inputs must be zero at fixed DOFs (tof_pack
+ * guarantees it).
+ *
+ * Element arrays are over the full nx*ny*nz grid, x fastest:
+ * e = (ez*ny + ey)*nx + ex.
+ *
+ * Citations are to the reference project (NinhGhoster/TO-F450-arm) by path
+ * within it.
+ */
+#ifndef TOF_H
+#define TOF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct tof_ctx tof_ctx;
+typedef struct tof_filter tof_filter;
+
+enum {
+  TOF_OK = 0,
+  TOF_NOT_CONVERGED = 1,
+  TOF_ERR_ARG = -1,
+  TOF_ERR_CUDA = -2,
+  TOF_ERR_BREAKDOWN = -3,
+  TOF_ERR_NONFINITE = -4,
+  TOF_ERR_TIMEOUT = -5
+};
+enum { TOF_OP_K = 0, TOF_OP_M = 1 };
+enum { TOF_F32 = 0, TOF_F64 = 1 };
+/* TOF_MODE_FP64: plain FP64 Jacobi PCG / FP64 LOBPCG (the drop-in form).
+ * TOF_MODE_MIXED: FP32 bulk arithmetic with FP64 iterative refinement (PCG)
+ * or a final FP64 Rayleigh-Ritz (LOBPCG). */
+enum { TOF_MODE_FP64 = 0, TOF_MODE_MIXED = 1 };
+enum { TOF_PRECOND_JACOBI = 0, TOF_PRECOND_PCG = 1 };
+enum { TOF_FILTER_FORWARD = 0, TOF_FILTER_ADJOINT = 1, TOF_FILTER_PHYSICAL = 2 };
+enum {
+  TOF_Q_NODES = 0, TOF_Q_ELEMS = 1, TOF_Q_FREE_DOFS = 2, TOF_Q_TILE_X = 3, TOF_Q_TILE_Y = 4,
+  TOF_Q_TILE_Z = 5, TOF_Q_DEVICE_BYTES = 6, TOF_Q_MAX_RHS = 7, TOF_Q_MAX_MODES = 8
+};
+
+typedef struct {
+  int status;     /* TOF_OK, TOF_NOT_CONVERGED or a TOF_ERR_* */
+  int iters;      /* Krylov / LOBPCG iterations (summed over refinement steps) */
+  int outer;      /* refinement steps (mixed PCG), else 1 */
+  double relres;  /* PCG: ||b - K x||_2 / ||b||_2 recomputed in FP64 at exit.
+                     LOBPCG: largest ||K x - theta M x|| / ||K x|| of the modes */
+} tof_solve_stats;
+
+/* SIMP interpolation constants: stiffness emin + (1-emin) rho^penal,
+ * mass rho for rho >= mass_threshold else t (rho/t)^mass_q.
+ * Reference: src/fem.py:204-205 (SIMP_PENALTY, E_MIN_FRAC), src/fem.py:331-349. */
+typedef struct {
+  double penal, emin, mass_threshold, mass_q;
+} tof_simp_params;
+
+int tof_version(void);
+const char* tof_last_error(const tof_ctx* ctx);   /* ctx may be NULL: last create error */
+
+/* Create a design context on the current CUDA device.
+ * Replaces FEM3D.__init__ (src/fem.py:207-308): the element matrices are the
+ * caller's 24x24 FP64 Ke / Me (src/fem.py:99-152; callers may overwrite them,
+ * e.g. orthotropic D), `active` marks in_arm voxels (NULL = all), `fixed_dof`
+ * (3*NN bytes, nonzero = clamped, src/fem.py:282-290) and the library adds
+ * ghost nodes of no active element itself (src/fem.py:292-305).  `tip_lump`
+ * (3*NN FP64 or NULL) is the lumped mass added to diag(M), i.e.
+ * mass_kg / n_nodes on each DOF of the tip nodes (src/fem.py:383-398).
+ * `tile` (node tile x, y, z; NULL = default 8x4x4) must have x*y*z <= 256.
+ * max_rhs / max_modes (1..8) size the solver workspace; this is the only
+ * call that allocates device memory. */
+int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[576], const double Me[576],
+                   const uint8_t* active, const uint8_t* fixed_dof, const double* tip_lump,
+                   const tof_simp_params* simp, int max_rhs, int max_modes, const int tile[3], tof_ctx** out);
+void tof_ctx_destroy(tof_ctx* ctx);
+long long tof_ctx_query(const tof_ctx* ctx, int what);
+
+/* Set element densities (device FP64 [NE]); computes SIMP stiffness and mass
+ * factors and the diagonals.  Replaces the per-call assemble_K / assemble_M
+ * (src/fem.py:311-398): no matrix is ever assembled. */
+int tof_set_density(tof_ctx* ctx, const double* rho, void* stream);
+
+/* Replace the lumped tip mass (host FP64 [3*NN], NULL = none) and refresh
+ * diag(M).  FEM3D.modal_analysis / eigenvalue_sensitivity take the tip mass
+ * per call (src/fem.py:400-435, 472-520); mass on fixed or ghost DOFs is
+ * dropped as the reference's K[free][:, free] slicing drops it. */
+int tof_set_tip_lump(tof_ctx* ctx, const double* tip_lump, void* stream);
+
+/* DOF-major FP64 (ld doubles between vectors) <-> node4 of dtype. */
+int tof_pack(tof_ctx* ctx, const double* src, long long ld, void* dst, int dtype, int nvec, void* stream);
+int tof_unpack(tof_ctx* ctx, const void* src, int dtype, double* dst, long long ld, int nvec, void* stream);
+
+/* y = A_ff x for A = K or M (matrix-free), nvec node4 vectors of dtype.
+ * The reference forms K[free][:, free] @ x from the assembled CSR
+ * (src/fem.py:437-438, src/fem_gpu.py:52-58). */
+int tof_matvec(tof_ctx* ctx, int op, int dtype, const void* x, void* y, int nvec, void* stream);
+
+/* diag(A_ff) as node4 FP64 (0 at fixed DOFs); src/fem.py:441-443, 543-544. */
+int tof_diag(tof_ctx* ctx, int op, double* out, void* stream);
+
+/* Solve K_ff u = b for nrhs node4 FP64 right-hand sides; x holds the start
+ * vectors on entry and the solution on exit.  Replaces
+ * FEM3D.apply_BCs_and_solve / FEM3D.solve (src/fem.py:529-561) and the GPU
+ * drop-in _solve_cg_gpu (src/fem_gpu.py:46-98); stops at
+ * ||b - K x||_2 <= rtol ||b||_2 like SciPy's cg.  Synchronises `stream`;
+ * stats (host, nrhs entries) may be NULL. */
+int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double rtol, int maxiter,
+            tof_solve_stats* stats, void* stream);
+
+/* Lowest `nmodes` eigenpairs of K_ff x = lam M_ff x with a block of `block`
+ * vectors (nmodes <= block <= 8).  X (device node4 FP64, `block` vectors)
+ * holds the start block on entry (warm start or random) and the
+ * M-orthonormal modes, ascending, in its first nmodes vectors on exit;
+ * lam (host, nmodes) gets the eigenvalues (rad/s)^2.  Replaces
+ * FEM3D.modal_analysis (src/fem.py:400-470) and _modal_gpu
+ * (src/fem_gpu.py:101-173).  precond: TOF_PRECOND_JACOBI (as the reference)
+ * or TOF_PRECOND_PCG (inner_iters pipelined PCG iterations to inner_rtol).
+ * Synchronises `stream`.  resid (host, nmodes) may be NULL. */
+int tof_lobpcg(tof_ctx* ctx, int mode, int nmodes, int block, double* X, double* lam, double tol, int maxiter,
+               int precond, int inner_iters, double inner_rtol, tof_solve_stats* stats, double* resid,
+               void* stream);
+
+/* Per-element quadratic forms v_e^T A_e v_e (A_e = Ke or Me, unscaled), FP64
+ * out [nvec][NE].  ce = u_e^T Ke u_e is FEM3D.elem_compliance
+ * (src/fem.py:605-615); phi_e^T Ke phi_e and phi_e^T Me phi_e are the
+ * contractions of FEM3D.eigenvalue_sensitivity (src/fem.py:498-501). */
+int tof_elem_quadform(tof_ctx* ctx, int op, int dtype, const void* v, int nvec, double* out, void* stream);
+
+/* G = A^T B (na x nb, row-major, device FP64) of node4 blocks, na, nb <= 24. */
+int tof_gram(tof_ctx* ctx, int dtype, const void* A, int na, const void* B, int nb, double* G, void* stream);
+
+/* Compliance and its sensitivity for nlc load cases from ce [nlc][NE]
+ * (src/topopt.py:291-306): c = sum_l w_l sum_e f_e ce_le (device scalar
+ * c_out), dc_e = sum_l w_l (-p (1-emin) rho_e^(p-1) ce_le) (device [NE]). */
+int tof_compliance_sens(tof_ctx* ctx, int nlc, const double* w, const double* ce, double* dc, double* c_out,
+                        void* stream);
+
+/* d lambda / d rho_e (device [NE]) for one mode from its quadratic forms
+ * qK, qM [NE] and the tip-mass term vMv_tip = m_node * sum(v_tip^2):
+ * FEM3D.eigenvalue_sensitivity (src/fem.py:472-526). */
+int tof_eig_sens(tof_ctx* ctx, const double* qK, const double* qM, double lam, double vMv_tip, double* out,
+                 void* stream);
+
+/* Effective-mass fractions (phi^T M r)^2 / (phi^T M phi) / (r^T M r) of
+ * nmodes node4 FP64 modes, r = unit translation along `direction` (0, 1, 2)
+ * on free DOFs; out (host, nmodes).  sims/modal_participation.py:37-57.
+ * Synchronises `stream`. */
+int tof_effective_mass(tof_ctx* ctx, const double* modes, int nmodes, int direction, double* out, void* stream);
+
+/* Density filter on an nx*ny*nz element grid (x fastest) with a (kx,ky,kz)
+ * weight array (z slowest: w[(qz*ky + qy)*kx + qx], odd sizes) and a mask
+ * (NE bytes).  Replaces topopt.cone_kernel / filter_field
+ * (src/topopt.py:32-58).  `fill` (NE bytes or NULL) marks active elements
+ * outside the mask that TOF_FILTER_PHYSICAL sets to 1
+ * (src/topopt.py:270-281). */
+int tof_filter_create(int nx, int ny, int nz, const double* w, int kx, int ky, int kz, const uint8_t* mask,
+                      const uint8_t* fill, tof_filter** out);
+int tof_filter_apply(tof_filter* f, int mode, const double* in, double* out, void* stream);
+void tof_filter_destroy(tof_filter* f);
+
+/* OC update with bisection on the Lagrange multiplier
+ * (SIMPOptimizer._oc_update, src/topopt.py:190-214); device FP64 arrays of
+ * n design cells; n_bisect (device int or NULL) gets the step count. */
+int tof_oc_update(int n, const double* x, const double* dc, double V_e, double target_volume, double move,
+                  double* x_new, int* n_bisect, void* stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOF_H */

@@ -84,9 +84,16 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Spin budget of every wait in this library: a wait that has not completed
-// after this many polls gives up, raises an error flag and returns.
-constexpr unsigned long long kSpinLimit = 1ull << 26;
+// Wait budget of every spin in this library: a wait that has not completed
+// after this long gives up, raises an error flag and returns (a legitimate
+// wait here lasts microseconds).
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
 
 // ----------------------------------------------------------------------------
 // Grid-wide barrier for persistent cooperative launches (all CTAs resident).
@@ -117,9 +124,10 @@ __device__ __forceinline__ bool grid_barrier(BarrierState* bs, unsigned nblocks)
       st_release_u32(&bs->gen, g + 1);
     } else {
       unsigned long long spins = 0;
+      const unsigned long long t0 = global_ns();
       while (ld_acquire_u32(&bs->gen) == g) {
         if (ld_relaxed_i32(&bs->error)) { ok = 0; break; }
-        if (++spins > kSpinLimit) {
+        if ((++spins & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
           atomicExch(&bs->error, ST_TIMEOUT);
           ok = 0;
           break;
@@ -149,7 +157,9 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
 // Bounded wait on phase `parity`; returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   uint32_t addr = smem_u32(bar);
-  for (unsigned long long i = 0; i < kSpinLimit; ++i) {
+  const unsigned long long t0 = global_ns();
+  for (unsigned long long i = 0;; ++i) {
+    if ((i & 1023) == 1023 && global_ns() - t0 > kWaitLimitNs) return false;
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

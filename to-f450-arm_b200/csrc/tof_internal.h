@@ -1,0 +1,100 @@
+// Host-side internals of libtof: the design context and kernel launchers.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "tof_common.cuh"
+
+namespace tof {
+
+struct SimpParams {
+  double penal = 3.0;          // SIMP exponent p (src/fem.py:204)
+  double emin = 1e-9;          // E_min / E (src/fem.py:205)
+  double mass_threshold = 0.1; // Pedersen threshold (src/fem.py:331)
+  double mass_q = 6.0;         // Pedersen exponent (src/fem.py:332)
+};
+
+// One design: grid, element matrices, boundary conditions, SIMP factors and
+// all solver workspace.  Everything is allocated in create(); solves never
+// allocate.
+struct Ctx {
+  int dev = 0;
+  int num_sms = 0;
+  Grid g{};
+  SimpParams sp{};
+  int max_rhs = 0, max_modes = 0;
+  int n_free = 0;
+
+  // element matrices (FP64 dense 24x24 and the 64-block layout, FP32/FP64)
+  double* Ke64 = nullptr; double* Me64 = nullptr;
+  double* keb64 = nullptr; double* meb64 = nullptr;
+  float* keb32 = nullptr; float* meb32 = nullptr;
+
+  uint8_t* active = nullptr;   // [NE]
+  uint8_t* fix = nullptr;      // [NN] bit c set: DOF c fixed (incl. ghost nodes)
+  double* tip64 = nullptr;     // node4 lumped tip mass (0 at fixed DOFs)
+  float* tip32 = nullptr;
+
+  // per-element factors
+  double *fK64 = nullptr, *fM64 = nullptr;
+  float *fK32 = nullptr, *fM32 = nullptr;
+  double* rho = nullptr;       // [NE] current density (0 outside the active set)
+  // diagonals and Jacobi inverses (node4)
+  double *dK64 = nullptr, *dM64 = nullptr, *dinvK64 = nullptr;
+  float *dinvK32 = nullptr;
+
+  // reductions / barrier
+  double* partials = nullptr;  // [max grid][64]
+  int partial_slots = 0;
+  BarrierState* bar = nullptr;
+  int* status = nullptr;       // [16] solver status words
+  double* scal = nullptr;      // [256] solver scalars
+
+  // PCG workspace
+  float* pw32 = nullptr;       // 10 node4 blocks of max_rhs vectors (FP32)
+  double* pw64 = nullptr;      // 7 node4 blocks of max_rhs vectors (FP64)
+  // LOBPCG workspace (FP32 node4): 2 sets x 3 blocks (S, KS, MS) of 3*max_modes
+  float* lw32 = nullptr;
+  double* lw64 = nullptr;      // FP64 refinement: X, KX, MX of max_modes
+  double* gram = nullptr;      // [2][24*24] + small-eig outputs
+  double* gram_part = nullptr; // [gram blocks][24*24]
+  int gram_blocks = 0;
+
+  // persistent-launch capacity for each kernel flavour
+  int coop_pipe[9] = {0};
+  int coop_plain[9] = {0};
+
+
+  std::vector<uint8_t> host_fix;   // host copy of `fix`
+  size_t bytes = 0;
+  std::string last_error;
+};
+
+// tensor-map encoding for a block of R node4 vectors (dtype float or double)
+bool encode_node4_map(CUtensorMap* m, const void* base, const Grid& g, int R, bool f64, std::string* err);
+
+// kernels (tof_kernels.cu)
+void launch_factors(Ctx& c, const double* rho, cudaStream_t s);
+void launch_diag(Ctx& c, cudaStream_t s);
+int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, const void* b_residual,
+                  cudaStream_t s);
+void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s);
+void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s);
+void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s);
+void launch_quadform(const Ctx& c, int op, bool f64, const void* v, int nvec, double* out, cudaStream_t s);
+void launch_convert(const void* src, bool src64, void* dst, bool dst64, long long n, cudaStream_t s);
+void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s);
+void launch_add_f32_to_f64(long long n, const float* d, double* x, cudaStream_t s);
+
+// PCG (tof_pcg.cu)
+int pcg_plain64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int* iters, double* relres,
+                int* status, cudaStream_t s);
+int pcg_pipe32(Ctx& c, const double* b, float* d, int R, double rtol, int maxiter, int* iters, double* relres,
+               int* status, cudaStream_t s);
+
+}  // namespace tof

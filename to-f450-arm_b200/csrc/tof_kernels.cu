@@ -1,0 +1,417 @@
+// Standalone (one-launch) kernels of the voxel SIMP path.
+#include <math.h>
+
+#include "tof_internal.h"
+#include "tof_stencil.cuh"
+
+namespace tof {
+
+// ---------------------------------------------------------------------------
+// SIMP factors.  Stiffness: emin + (1 - emin) rho^p (src/fem.py:316-320).
+// Mass (Pedersen): rho for rho >= t, t (max(rho,0)/t)^q below
+// (src/fem.py:334-349).  Elements outside the active set get 0 (they are not
+// part of the reference's assembly at all).
+// ---------------------------------------------------------------------------
+__global__ void k_factors(int NE, const double* __restrict__ rho, const uint8_t* __restrict__ active,
+                          SimpParams sp, double* fK64, double* fM64, float* fK32, float* fM32) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= NE) return;
+  double fk = 0.0, fm = 0.0;
+  if (active[e]) {
+    const double r = rho[e];
+    fk = sp.emin + (1.0 - sp.emin) * pow(r, sp.penal);
+    fm = (r >= sp.mass_threshold) ? r : sp.mass_threshold * pow(fmax(r, 0.0) / sp.mass_threshold, sp.mass_q);
+  }
+  fK64[e] = fk; fM64[e] = fm;
+  fK32[e] = float(fk); fM32[e] = float(fm);
+}
+
+void launch_factors(Ctx& c, const double* rho, cudaStream_t s) {
+  const int NE = c.g.NE;
+  k_factors<<<ceil_div(NE, 256), 256, 0, s>>>(NE, rho, c.active, c.sp, c.fK64, c.fM64, c.fK32, c.fM32);
+}
+
+// ---------------------------------------------------------------------------
+// Diagonals of K and M (node4) and the Jacobi inverse of diag K.  Fixed DOFs
+// get diag 0 and inverse 0, so preconditioned vectors stay zero there.  The
+// reference's Jacobi preconditioner is 1 / diag(K_ff) (src/fem.py:543-544).
+// ---------------------------------------------------------------------------
+__global__ void k_diag(Grid g, const double* __restrict__ fK, const double* __restrict__ fM,
+                       const double* __restrict__ Ke, const double* __restrict__ Me,
+                       const uint8_t* __restrict__ fix, const double* __restrict__ tip, double* dK, double* dM,
+                       double* dinv64, float* dinv32) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= g.NN) return;
+  const int i = n % g.NX, j = (n / g.NX) % g.NY, k = n / (g.NX * g.NY);
+  double sk[3] = {0, 0, 0}, sm[3] = {0, 0, 0};
+  for (int c = -1; c <= 0; ++c)
+    for (int b = -1; b <= 0; ++b)
+      for (int a = -1; a <= 0; ++a) {
+        const int ex = i + a, ey = j + b, ez = k + c;
+        if (ex < 0 || ey < 0 || ez < 0 || ex >= g.nx || ey >= g.ny || ez >= g.nz) continue;
+        const int e = (ez * g.ny + ey) * g.nx + ex;
+        const int ln = local_node(-a, -b, -c);
+        for (int q = 0; q < 3; ++q) {
+          const int d = (3 * ln + q) * 24 + 3 * ln + q;
+          sk[q] += fK[e] * Ke[d];
+          sm[q] += fM[e] * Me[d];
+        }
+      }
+  const uint8_t fx = fix[n];
+  for (int q = 0; q < 3; ++q) {
+    const bool fixed = (fx >> q) & 1;
+    const double kq = fixed ? 0.0 : sk[q];
+    const double mq = fixed ? 0.0 : sm[q] + tip[4 * n + q];
+    dK[4 * n + q] = kq;
+    dM[4 * n + q] = mq;
+    const double inv = (fixed || kq == 0.0) ? 0.0 : 1.0 / kq;
+    dinv64[4 * n + q] = inv;
+    dinv32[4 * n + q] = float(inv);
+  }
+  dK[4 * n + 3] = dM[4 * n + 3] = dinv64[4 * n + 3] = 0.0;
+  dinv32[4 * n + 3] = 0.f;
+}
+
+void launch_diag(Ctx& c, cudaStream_t s) {
+  k_diag<<<ceil_div(c.g.NN, 256), 256, 0, s>>>(c.g, c.fK64, c.fM64, c.Ke64, c.Me64, c.fix, c.tip64, c.dK64,
+                                                 c.dM64, c.dinvK64, c.dinvK32);
+}
+
+// ---------------------------------------------------------------------------
+// Standalone block matvec: y = A x (or y = b - A x) for R node4 vectors, one
+// node tile per CTA.  Input vectors must be zero at fixed DOFs (pack()
+// guarantees that).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct MatvecArgs {
+  Grid g;
+  const T* fe;         // element factors
+  const T* keb;        // 64-block matrix
+  const uint8_t* fix;
+  const T* tip;        // node4 lumped mass (M only) or null
+  const T* b;          // residual mode: rhs, else null
+  T* y;
+  long long vstride;   // elements between consecutive vectors (NN*4)
+};
+
+template <typename T, int R>
+__global__ void __launch_bounds__(512) k_matvec(const __grid_constant__ CUtensorMap tmx, MatvecArgs<T> a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  using V4 = typename Vec4<T>::type;
+  const Grid& g = a.g;
+  const TileGeom tg = tile_geom(g, blockIdx.x);
+  T* sx = reinterpret_cast<T*>(smem_raw);
+  const unsigned hb = halo_bytes<T>(g, R);
+  T* sKe = reinterpret_cast<T*>(smem_raw + hb);
+  T* sf = sKe + kKeBlocksLen;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((hb + sizeof(T) * (kKeBlocksLen + tg.EX * tg.EY * tg.EZ) + 15) & ~15u));
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, hb);
+    tma_load_5d(sx, &tmx, 0, tg.i0 - 1, tg.j0 - 1, tg.k0 - 1, 0, bar);
+  }
+  load_ke_blocks(a.keb, sKe);
+  load_factor_tile(g, tg, a.fe, sf);
+  __syncthreads();
+  if (!mbar_wait(bar, 0)) return;
+  int tx, ty, tz, n;
+  if (!thread_node(g, tg, tx, ty, tz, n)) return;
+  T acc[R][3];
+  stencil_node<T, R>(sx, tg, sf, sKe, tx, ty, tz, acc);
+  const uint8_t fx = __ldg(a.fix + n);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (a.tip) {
+      const V4 xc = halo_center<T>(sx, tg, r, tx, ty, tz);
+      const V4 tp = reinterpret_cast<const V4*>(a.tip)[n];
+      acc[r][0] = fma(tp.x, xc.x, acc[r][0]);
+      acc[r][1] = fma(tp.y, xc.y, acc[r][1]);
+      acc[r][2] = fma(tp.z, xc.z, acc[r][2]);
+    }
+    V4 out;
+    if (a.b) {
+      const V4 bb = reinterpret_cast<const V4*>(a.b + r * a.vstride)[n];
+      out.x = bb.x - acc[r][0]; out.y = bb.y - acc[r][1]; out.z = bb.z - acc[r][2];
+    } else {
+      out.x = acc[r][0]; out.y = acc[r][1]; out.z = acc[r][2];
+    }
+    out.x = (fx & 1) ? T(0) : out.x;
+    out.y = (fx & 2) ? T(0) : out.y;
+    out.z = (fx & 4) ? T(0) : out.z;
+    out.w = T(0);
+    reinterpret_cast<V4*>(a.y + r * a.vstride)[n] = out;
+  }
+}
+
+template <typename T, int R>
+static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b, cudaStream_t s) {
+  CUtensorMap tm;
+  std::string err;
+  if (!encode_node4_map(&tm, x, c.g, R, sizeof(T) == 8, &err)) {
+    c.last_error = err;
+    return -2;
+  }
+  MatvecArgs<T> a;
+  a.g = c.g;
+  const bool f64 = sizeof(T) == 8;
+  a.fe = reinterpret_cast<const T*>(op == 0 ? (f64 ? (const void*)c.fK64 : (const void*)c.fK32)
+                                            : (f64 ? (const void*)c.fM64 : (const void*)c.fM32));
+  a.keb = reinterpret_cast<const T*>(op == 0 ? (f64 ? (const void*)c.keb64 : (const void*)c.keb32)
+                                             : (f64 ? (const void*)c.meb64 : (const void*)c.meb32));
+  a.fix = c.fix;
+  a.tip = op == 1 ? reinterpret_cast<const T*>(f64 ? (const void*)c.tip64 : (const void*)c.tip32) : nullptr;
+  a.b = reinterpret_cast<const T*>(b);
+  a.y = reinterpret_cast<T*>(y);
+  a.vstride = (long long)c.g.NN * 4;
+  const TileGeom tg{0, 0, 0, c.g.TX + 2, c.g.TY + 2, c.g.TZ + 2, c.g.TX + 1, c.g.TY + 1, c.g.TZ + 1};
+  size_t smem = halo_bytes<T>(c.g, R) + sizeof(T) * (kKeBlocksLen + tg.EX * tg.EY * tg.EZ);
+  smem = ((smem + 15) & ~size_t(15)) + 16;
+  auto kern = k_matvec<T, R>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<c.g.ntiles, c.g.TX * c.g.TY * c.g.TZ, smem, s>>>(tm, a);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, const void* b, cudaStream_t s) {
+  // split into chunks of at most 8 vectors
+  const size_t esz = f64 ? 8 : 4;
+  const long long vbytes = (long long)c.g.NN * 4 * esz;
+  int done = 0;
+  while (done < nrhs) {
+    int R = nrhs - done;
+    R = R >= 8 ? 8 : R >= 4 ? 4 : R >= 2 ? 2 : 1;
+    const char* xp = (const char*)x + done * vbytes;
+    char* yp = (char*)y + done * vbytes;
+    const char* bp = b ? (const char*)b + done * vbytes : nullptr;
+    int rc;
+    if (f64) {
+      switch (R) {
+        case 8: rc = matvec_launch_t<double, 8>(c, op, xp, yp, bp, s); break;
+        case 4: rc = matvec_launch_t<double, 4>(c, op, xp, yp, bp, s); break;
+        case 2: rc = matvec_launch_t<double, 2>(c, op, xp, yp, bp, s); break;
+        default: rc = matvec_launch_t<double, 1>(c, op, xp, yp, bp, s); break;
+      }
+    } else {
+      switch (R) {
+        case 8: rc = matvec_launch_t<float, 8>(c, op, xp, yp, bp, s); break;
+        case 4: rc = matvec_launch_t<float, 4>(c, op, xp, yp, bp, s); break;
+        case 2: rc = matvec_launch_t<float, 2>(c, op, xp, yp, bp, s); break;
+        default: rc = matvec_launch_t<float, 1>(c, op, xp, yp, bp, s); break;
+      }
+    }
+    if (rc) return rc;
+    done += R;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// DOF-major (the reference's 3*n + c layout) <-> node4, with the fixed-DOF
+// restriction applied on the way in.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_pack(int NN, int nvec, const double* __restrict__ src, long long ld, const uint8_t* fix, T* dst) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)NN * nvec) return;
+  const int v = int(idx / NN), n = int(idx % NN);
+  const double* s = src + v * ld + 3 * (long long)n;
+  const uint8_t fx = fix[n];
+  typename Vec4<T>::type o;
+  o.x = (fx & 1) ? T(0) : T(s[0]);
+  o.y = (fx & 2) ? T(0) : T(s[1]);
+  o.z = (fx & 4) ? T(0) : T(s[2]);
+  o.w = T(0);
+  reinterpret_cast<typename Vec4<T>::type*>(dst)[idx] = o;
+}
+
+template <typename T>
+__global__ void k_unpack(int NN, int nvec, const T* __restrict__ src, double* dst, long long ld) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)NN * nvec) return;
+  const int v = int(idx / NN), n = int(idx % NN);
+  const typename Vec4<T>::type i = reinterpret_cast<const typename Vec4<T>::type*>(src)[idx];
+  double* d = dst + v * ld + 3 * (long long)n;
+  d[0] = double(i.x); d[1] = double(i.y); d[2] = double(i.z);
+}
+
+void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s) {
+  const long long n = (long long)c.g.NN * nvec;
+  const int blocks = int((n + 255) / 256);
+  if (f64) k_pack<double><<<blocks, 256, 0, s>>>(c.g.NN, nvec, src, ld, c.fix, (double*)dst);
+  else k_pack<float><<<blocks, 256, 0, s>>>(c.g.NN, nvec, src, ld, c.fix, (float*)dst);
+}
+
+void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s) {
+  const long long n = (long long)c.g.NN * nvec;
+  const int blocks = int((n + 255) / 256);
+  if (f64) k_unpack<double><<<blocks, 256, 0, s>>>(c.g.NN, nvec, (const double*)src, dst, ld);
+  else k_unpack<float><<<blocks, 256, 0, s>>>(c.g.NN, nvec, (const float*)src, dst, ld);
+}
+
+// ---------------------------------------------------------------------------
+// Gram matrix G = A^T B of two blocks of node4 vectors (na, nb <= 24) with
+// FP64 accumulation.  Stage 1: each CTA reduces a contiguous range of node
+// chunks into a partial matrix; stage 2 sums the partials in block order
+// (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kGramThreads = 256;
+constexpr int kGramMaxPerThread = 3;   // 24*24 = 576 <= 3*256 - 192
+
+template <typename T, int CH>
+__global__ void __launch_bounds__(kGramThreads) k_gram_partial(int NN, const T* __restrict__ A, int na,
+                                                              const T* __restrict__ B, int nb, long long vstride,
+                                                              double* part) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ V4 sA[24 * CH];
+  __shared__ V4 sB[24 * CH];
+  const int npair = na * nb;
+  double acc[kGramMaxPerThread] = {0, 0, 0};
+  const int nchunks = (NN + CH - 1) / CH;
+  const int per = (nchunks + gridDim.x - 1) / gridDim.x;
+  const int c0 = blockIdx.x * per, c1 = min(nchunks, c0 + per);
+  for (int ch = c0; ch < c1; ++ch) {
+    const int n0 = ch * CH;
+    const int cnt = min(CH, NN - n0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < na * CH; idx += blockDim.x) {
+      const int v = idx / CH, q = idx % CH;
+      V4 z{};
+      sA[idx] = q < cnt ? reinterpret_cast<const V4*>(A + v * vstride)[n0 + q] : z;
+    }
+    for (int idx = threadIdx.x; idx < nb * CH; idx += blockDim.x) {
+      const int v = idx / CH, q = idx % CH;
+      V4 z{};
+      sB[idx] = q < cnt ? reinterpret_cast<const V4*>(B + v * vstride)[n0 + q] : z;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < kGramMaxPerThread; ++t) {
+      const int p = threadIdx.x + t * kGramThreads;
+      if (p < npair) {
+        const int ia = p / nb, ib = p % nb;
+        const V4* a = sA + ia * CH;
+        const V4* b = sB + ib * CH;
+        double s = 0.0;
+        for (int q = 0; q < cnt; ++q) {
+          const V4 x = a[q], y = b[q];
+          s = fma(double(x.x), double(y.x), s);
+          s = fma(double(x.y), double(y.y), s);
+          s = fma(double(x.z), double(y.z), s);
+        }
+        acc[t] += s;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < kGramMaxPerThread; ++t) {
+    const int p = threadIdx.x + t * kGramThreads;
+    if (p < npair) part[(size_t)blockIdx.x * 576 + p] = acc[t];
+  }
+}
+
+__global__ void k_gram_reduce(int nblocks, int npair, const double* __restrict__ part, double* G) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npair) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * 576 + p];
+  G[p] = s;
+}
+
+void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s) {
+  const int CH = f64 ? 16 : 32;
+  const int nchunks = ceil_div(c.g.NN, CH);
+  int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
+  if (blocks < 1) blocks = 1;
+  const long long vs = (long long)c.g.NN * 4;
+  if (f64)
+    k_gram_partial<double, 16><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, na, (const double*)B, nb,
+                                                               vs, c.gram_part);
+  else
+    k_gram_partial<float, 32><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, na, (const float*)B, nb,
+                                                              vs, c.gram_part);
+  k_gram_reduce<<<ceil_div(na * nb, 128), 128, 0, s>>>(blocks, na * nb, c.gram_part, G);
+}
+
+// ---------------------------------------------------------------------------
+// Element quadratic forms q_e = v_e^T A v_e (A = Ke or Me) for nvec vectors,
+// FP64 accumulation.  ce = u_e^T Ke u_e is src/fem.py:605-615; the eigenvalue
+// sensitivity's phi_e^T Ke phi_e and phi_e^T Me phi_e are src/fem.py:499-501.
+// Output [nvec][NE] over the full element grid (x fastest); 0 for inactive
+// elements.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_quadform(Grid g, const T* __restrict__ v, int nvec, long long vstride,
+                                                  const double* __restrict__ Ae, const uint8_t* __restrict__ active,
+                                                  double* out) {
+  __shared__ double sA[576];
+  for (int i = threadIdx.x; i < 576; i += blockDim.x) sA[i] = Ae[i];
+  __syncthreads();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= g.NE) return;
+  const int ex = e % g.nx, ey = (e / g.nx) % g.ny, ez = e / (g.nx * g.ny);
+  const bool act = active[e] != 0;
+  for (int r = 0; r < nvec; ++r) {
+    double ue[24];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+      const int ox = (l == 1 || l == 2 || l == 5 || l == 6) ? 1 : 0;
+      const int oy = (l == 2 || l == 3 || l == 6 || l == 7) ? 1 : 0;
+      const int oz = l >= 4 ? 1 : 0;
+      const int n = ((ez + oz) * g.NY + (ey + oy)) * g.NX + (ex + ox);
+      const typename Vec4<T>::type x = reinterpret_cast<const typename Vec4<T>::type*>(v + r * vstride)[n];
+      ue[3 * l] = double(x.x); ue[3 * l + 1] = double(x.y); ue[3 * l + 2] = double(x.z);
+    }
+    double q = 0.0;
+#pragma unroll 4
+    for (int i = 0; i < 24; ++i) {
+      double t = 0.0;
+#pragma unroll
+      for (int j = 0; j < 24; ++j) t = fma(sA[i * 24 + j], ue[j], t);
+      q = fma(ue[i], t, q);
+    }
+    out[(size_t)r * g.NE + e] = act ? q : 0.0;
+  }
+}
+
+void launch_quadform(const Ctx& c, int op, bool f64, const void* v, int nvec, double* out, cudaStream_t s) {
+  const double* A = op == 0 ? c.Ke64 : c.Me64;
+  const long long vs = (long long)c.g.NN * 4;
+  const int blocks = ceil_div(c.g.NE, 256);
+  if (f64) k_quadform<double><<<blocks, 256, 0, s>>>(c.g, (const double*)v, nvec, vs, A, c.active, out);
+  else k_quadform<float><<<blocks, 256, 0, s>>>(c.g, (const float*)v, nvec, vs, A, c.active, out);
+}
+
+// ---------------------------------------------------------------------------
+// small vector helpers
+// ---------------------------------------------------------------------------
+template <typename S, typename D>
+__global__ void k_convert(const S* __restrict__ src, D* dst, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = D(src[i]);
+}
+
+void launch_convert(const void* src, bool src64, void* dst, bool dst64, long long n, cudaStream_t s) {
+  const int blocks = int((n + 255) / 256);
+  if (src64 && !dst64) k_convert<double, float><<<blocks, 256, 0, s>>>((const double*)src, (float*)dst, n);
+  else if (!src64 && dst64) k_convert<float, double><<<blocks, 256, 0, s>>>((const float*)src, (double*)dst, n);
+  else if (src64) k_convert<double, double><<<blocks, 256, 0, s>>>((const double*)src, (double*)dst, n);
+  else k_convert<float, float><<<blocks, 256, 0, s>>>((const float*)src, (float*)dst, n);
+}
+
+__global__ void k_axpy64(long long n, const double* __restrict__ x, double* y, double a) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = fma(a, x[i], y[i]);
+}
+void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s) {
+  k_axpy64<<<int((n + 255) / 256), 256, 0, s>>>(n, x, y, a);
+}
+
+__global__ void k_add_f32_to_f64(long long n, const float* __restrict__ d, double* x) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) x[i] += double(d[i]);
+}
+void launch_add_f32_to_f64(long long n, const float* d, double* x, cudaStream_t s) {
+  k_add_f32_to_f64<<<int((n + 255) / 256), 256, 0, s>>>(n, d, x);
+}
+
+}  // namespace tof

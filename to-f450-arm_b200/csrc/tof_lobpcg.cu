@@ -1,0 +1,428 @@
+// Block LOBPCG for the lowest modes of K x = lambda M x (sm_100a).
+//
+// The reference calls SciPy's lobpcg on the assembled K_ff, M_ff with a Jacobi
+// preconditioner, tol 1e-4, maxiter 500 (src/fem.py:400-470; CuPy's lobpcg
+// on the GPU, src/fem_gpu.py:101-173).  Here the block vectors live on the
+// device in node4 layout; each iteration:
+//   W = K X - M X diag(theta)           (k_lob_resid, FP64 norms)
+//   W <- T W                            (Jacobi, or a few pipelined block-PCG
+//                                        iterations on K: inexact K^-1)
+//   KW, MW                              (matrix-free block matvecs)
+//   G_K = S^T K S, G_M = S^T M S        (S = [X W P], FP64 Gram)
+//   Rayleigh-Ritz on (G_K, G_M)         (k_small_eig: one warp, FP64 Jacobi,
+//                                        basis conditioning by eigen-
+//                                        decomposition of the scaled G_M)
+//   X, P, KX, MX, KP, MP <- S C         (k_lob_update)
+// In mixed mode the block vectors are FP32 and a final FP64 Rayleigh-Ritz on
+// freshly computed FP64 K X, M X gives the eigenvalues; in FP64 mode
+// everything is FP64.
+#include <math.h>
+
+#include "tof_internal.h"
+#include "tof_stencil.cuh"
+
+namespace tof {
+
+constexpr int kMaxBasis = 24;
+
+// ---------------------------------------------------------------------------
+// residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, and per-CTA
+// partial sums of ||W_j||^2 and ||KX_j||^2 (unscaled residual)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs, const T* __restrict__ KX,
+                                                   const T* __restrict__ MX, const double* __restrict__ theta,
+                                                   const T* __restrict__ dinv, T* W, double* part) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ double red[2 * 8 * 32];
+  double v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = 0.0;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
+    V4 di;
+    if (dinv) di = reinterpret_cast<const V4*>(dinv)[n];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (j >= nb) break;
+      const size_t o = j * vs / 4 + n;
+      const V4 kx = reinterpret_cast<const V4*>(KX)[o];
+      const V4 mx = reinterpret_cast<const V4*>(MX)[o];
+      const T th = T(theta[j]);
+      V4 w;
+      w.x = kx.x - th * mx.x; w.y = kx.y - th * mx.y; w.z = kx.z - th * mx.z; w.w = T(0);
+      v[2 * j] += double(w.x) * w.x + double(w.y) * w.y + double(w.z) * w.z;
+      v[2 * j + 1] += double(kx.x) * kx.x + double(kx.y) * kx.y + double(kx.z) * kx.z;
+      if (dinv) { w.x *= di.x; w.y *= di.y; w.z *= di.z; }
+      reinterpret_cast<V4*>(W)[o] = w;
+    }
+  }
+  block_sum<16>(v, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 16; ++k) part[(size_t)blockIdx.x * 16 + k] = v[k];
+}
+
+__global__ void k_lob_resid_reduce(int nblk, const double* __restrict__ part, double* out) {
+  const int k = threadIdx.x;
+  if (k >= 16) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[(size_t)b * 16 + k];
+  out[k] = s;
+}
+
+// ---------------------------------------------------------------------------
+// One-warp parallel cyclic Jacobi eigensolver for a symmetric n x n (n <= 24)
+// matrix held in shared memory.  Round-robin ordering applies n/2 disjoint
+// rotations per step (rows, then columns, then the eigenvector matrix).
+// Rotation: Golub & Van Loan, Matrix Computations, Alg. 8.4.1 (sym.schur2).
+// ---------------------------------------------------------------------------
+constexpr int LDA = kMaxBasis + 1;
+
+__device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane) {
+  const int np = n + (n & 1);
+  for (int w = lane; w < np * np; w += 32) {
+    const int i = w / np, j = w % np;
+    V[i][j] = (i == j) ? 1.0 : 0.0;
+    if (i >= n || j >= n) A[i][j] = (i == j) ? 0.0 : 0.0;
+  }
+  __syncwarp();
+  __shared__ double cs_s[kMaxBasis / 2], sn_s[kMaxBasis / 2];
+  __shared__ int P_s[kMaxBasis / 2], Q_s[kMaxBasis / 2];
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int w = lane; w < n * n; w += 32) {
+      const int i = w / n, j = w % n;
+      const double a = A[i][j];
+      tot += a * a;
+      if (i != j) off += a * a;
+    }
+    off = warp_sum(off);
+    tot = warp_sum(tot);
+    if (!(off > 1e-30 * tot) || np < 2) break;
+    for (int r = 0; r < np - 1; ++r) {
+      if (lane < np / 2) {
+        const int k = lane;
+        auto pos = [&](int q) { return q == 0 ? 0 : 1 + ((q - 1 + r) % (np - 1)); };
+        int p = pos(k), q = pos(np - 1 - k);
+        if (p > q) { const int t = p; p = q; q = t; }
+        double c = 1.0, s = 0.0;
+        if (q < n) {
+          const double apq = A[p][q];
+          if (apq != 0.0) {
+            const double tau = (A[q][q] - A[p][p]) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        P_s[k] = p; Q_s[k] = q; cs_s[k] = c; sn_s[k] = s;
+      }
+      __syncwarp();
+      const int npair = np / 2;
+      // rows: A <- J^T A
+      for (int w = lane; w < npair * np; w += 32) {
+        const int k = w / np, j = w % np;
+        const int p = P_s[k], q = Q_s[k];
+        const double c = cs_s[k], s = sn_s[k];
+        const double ap = A[p][j], aq = A[q][j];
+        A[p][j] = c * ap - s * aq;
+        A[q][j] = s * ap + c * aq;
+      }
+      __syncwarp();
+      // columns: A <- A J ; V <- V J
+      for (int w = lane; w < npair * np; w += 32) {
+        const int k = w / np, j = w % np;
+        const int p = P_s[k], q = Q_s[k];
+        const double c = cs_s[k], s = sn_s[k];
+        const double ap = A[j][p], aq = A[j][q];
+        A[j][p] = c * ap - s * aq;
+        A[j][q] = s * ap + c * aq;
+        const double vp = V[j][p], vq = V[j][q];
+        V[j][p] = c * vp - s * vq;
+        V[j][q] = s * vp + c * vq;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Rayleigh-Ritz: the m smallest eigenpairs of G_K c = theta G_M c (n x n).
+// G_M is scaled to unit diagonal and eigendecomposed; directions with
+// eigenvalue below drop_tol * max are discarded (a near-dependent basis), and
+// the standard problem is solved in the remaining orthonormal basis.
+// Outputs: C (n x m, row-major), theta (m), info[0] = kept rank (or -1).
+__global__ void k_small_eig(int n, int m, const double* __restrict__ GK, const double* __restrict__ GM,
+                            double drop_tol, double* C, double* theta, int* info) {
+  __shared__ double A[kMaxBasis][LDA], B[kMaxBasis][LDA], V[kMaxBasis][LDA], Z[kMaxBasis][LDA];
+  __shared__ double D[kMaxBasis], ev[kMaxBasis];
+  __shared__ int keep[kMaxBasis], order[kMaxBasis];
+  __shared__ int kr;
+  const int lane = threadIdx.x;
+  for (int w = lane; w < n; w += 32) {
+    const double b = GM[w * n + w];
+    D[w] = b > 0.0 ? 1.0 / sqrt(b) : 0.0;
+  }
+  __syncwarp();
+  for (int w = lane; w < n * n; w += 32) {
+    const int i = w / n, j = w % n;
+    A[i][j] = 0.5 * (GK[i * n + j] + GK[j * n + i]) * D[i] * D[j];
+    B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
+  }
+  __syncwarp();
+  warp_jacobi(B, V, n, lane);
+  // kept directions of the basis
+  if (lane == 0) {
+    double bmax = 0.0;
+    for (int i = 0; i < n; ++i) bmax = fmax(bmax, B[i][i]);
+    int k = 0;
+    for (int i = 0; i < n; ++i)
+      if (D[i] > 0.0 && B[i][i] > drop_tol * bmax) keep[k++] = i;
+    kr = k;
+  }
+  __syncwarp();
+  const int K = kr;
+  // Z = V[:, keep] / sqrt(lambda)
+  for (int w = lane; w < n * K; w += 32) {
+    const int i = w / K, a = w % K;
+    Z[i][a] = V[i][keep[a]] / sqrt(B[keep[a]][keep[a]]);
+  }
+  __syncwarp();
+  // V <- A Z  (n x K), then B <- Z^T V (K x K)
+  for (int w = lane; w < n * K; w += 32) {
+    const int i = w / K, a = w % K;
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s = fma(A[i][j], Z[j][a], s);
+    V[i][a] = s;
+  }
+  __syncwarp();
+  for (int w = lane; w < K * K; w += 32) {
+    const int a = w / K, b = w % K;
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s = fma(Z[j][a], V[j][b], s);
+    B[a][b] = s;
+  }
+  __syncwarp();
+  for (int w = lane; w < K * K; w += 32) {
+    const int a = w / K, b = w % K;
+    A[a][b] = 0.5 * (B[a][b] + B[b][a]);
+  }
+  __syncwarp();
+  warp_jacobi(A, V, K, lane);
+  if (lane == 0) {
+    for (int i = 0; i < K; ++i) { ev[i] = A[i][i]; order[i] = i; }
+    for (int i = 0; i < K; ++i)
+      for (int j = i + 1; j < K; ++j)
+        if (ev[order[j]] < ev[order[i]]) { const int t = order[i]; order[i] = order[j]; order[j] = t; }
+    info[0] = K >= m ? K : -1;
+  }
+  __syncwarp();
+  if (K < m) return;
+  for (int w = lane; w < m; w += 32) theta[w] = ev[order[w]];
+  // C = D Z U[:, order[:m]]
+  for (int w = lane; w < n * m; w += 32) {
+    const int i = w / m, k = w % m;
+    double s = 0.0;
+    for (int a = 0; a < K; ++a) s = fma(Z[i][a], V[a][order[k]], s);
+    C[i * m + k] = D[i] * s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block update: Xn = S C, Pn = S[:, nb:] C[nb:, :] for S, KS, MS
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, long long vs,
+                                                    const T* __restrict__ S, const T* __restrict__ KS,
+                                                    const T* __restrict__ MS, const double* __restrict__ C,
+                                                    T* S2, T* KS2, T* MS2) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ T sC[kMaxBasis * 8];
+  for (int i = threadIdx.x; i < ncols * nb; i += blockDim.x) sC[i] = T(C[i]);
+  __syncthreads();
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= NN) return;
+  const T* src[3] = {S, KS, MS};
+  T* dst[3] = {S2, KS2, MS2};
+#pragma unroll 1
+  for (int b = 0; b < 3; ++b) {
+    V4 in[kMaxBasis];
+#pragma unroll
+    for (int j = 0; j < kMaxBasis; ++j)
+      if (j < ncols) in[j] = reinterpret_cast<const V4*>(src[b])[j * vs / 4 + n];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k >= nb) break;
+      V4 x{}, p{};
+#pragma unroll
+      for (int j = 0; j < kMaxBasis; ++j) {
+        if (j < ncols) {
+          const T c = sC[j * nb + k];
+          x.x = fma(c, in[j].x, x.x); x.y = fma(c, in[j].y, x.y); x.z = fma(c, in[j].z, x.z);
+          if (j >= nb) { p.x = fma(c, in[j].x, p.x); p.y = fma(c, in[j].y, p.y); p.z = fma(c, in[j].z, p.z); }
+        }
+      }
+      x.w = T(0); p.w = T(0);
+      reinterpret_cast<V4*>(dst[b])[k * vs / 4 + n] = x;
+      reinterpret_cast<V4*>(dst[b])[(2 * nb + k) * vs / 4 + n] = p;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+struct LobBufs {
+  void* S[2];
+  void* KS[2];
+  void* MS[2];
+};
+
+template <typename T>
+static inline T* vec(void* base, int j, long long vs) {
+  return reinterpret_cast<T*>(base) + j * vs;
+}
+
+static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s) {
+  double* GK = c.gram;
+  double* GM = c.gram + 576;
+  double* C = c.gram + 2 * 576;
+  double* th = c.gram + 3 * 576;
+  int* info = c.status + 8;
+  k_small_eig<<<1, 32, 0, s>>>(n, m, GK, GM, drop, C, th, info);
+  return 0;
+}
+
+int lobpcg_run(Ctx& c, bool f64, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter,
+               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, int verbose,
+               cudaStream_t s);
+
+// Implementation templated on the vector type.
+template <typename T>
+static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter, int precond,
+                       int inner_iters, double inner_rtol, int* iters_out, double* resid_out, cudaStream_t s) {
+  const bool f64 = sizeof(T) == 8;
+  const long long vs = (long long)c.g.NN * 4;
+  const int NN = c.g.NN;
+  const long long blk = 3LL * c.max_modes * vs;   // one S / KS / MS block (elements)
+  T* base = f64 ? reinterpret_cast<T*>(c.lw64 + 3 * (long long)c.max_modes * vs)
+                : reinterpret_cast<T*>(c.lw32);
+  LobBufs B;
+  for (int q = 0; q < 2; ++q) {
+    B.S[q] = base + (3 * q + 0) * blk;
+    B.KS[q] = base + (3 * q + 1) * blk;
+    B.MS[q] = base + (3 * q + 2) * blk;
+  }
+  const double drop = f64 ? 1e-12 : 1e-9;
+  double* GK = c.gram;
+  double* GM = c.gram + 576;
+  double* C = c.gram + 2 * 576;
+  double* th = c.gram + 3 * 576;
+  double* rn = c.gram + 3 * 576 + 32;
+  int* info = c.status + 8;
+  const int rblocks = 2 * c.num_sms;
+  int cur = 0;
+  // X <- X64 (first nb vectors), KX, MX
+  launch_convert(X64, true, B.S[cur], f64, (long long)nb * vs, s);
+  if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
+  if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
+  // initial Rayleigh-Ritz on X alone
+  launch_gram(c, f64, B.S[cur], nb, B.KS[cur], nb, GK, s);
+  launch_gram(c, f64, B.S[cur], nb, B.MS[cur], nb, GM, s);
+  lob_small_eig(c, nb, nb, drop, s);
+  k_lob_update<T><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, nb, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
+                                                     (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1]);
+  cur ^= 1;
+  int it = 0;
+  double hr[16];
+  double hth[8];
+  int hinfo = 0;
+  cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  if (hinfo < 0) { c.last_error = "LOBPCG: initial block is rank deficient"; return -3; }
+  bool conv = false;
+  for (it = 0; it < maxiter; ++it) {
+    T* X = (T*)B.S[cur];
+    T* W = vec<T>(B.S[cur], nb, vs);
+    const T* dinv = nullptr;
+    if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
+    k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, W, c.gram_part);
+    k_lob_resid_reduce<<<1, 32, 0, s>>>(rblocks, c.gram_part, rn);
+    cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
+    double worst = 0.0;
+    bool finite = true;
+    for (int j = 0; j < nmodes; ++j) {
+      const double r = sqrt(hr[2 * j]) / fmax(sqrt(hr[2 * j + 1]), 1e-300);
+      if (!isfinite(r)) finite = false;
+      worst = fmax(worst, r);
+      if (resid_out) resid_out[j] = r;
+    }
+    if (hinfo < 0) { c.last_error = "LOBPCG: Rayleigh-Ritz basis rank deficient"; return -3; }
+    if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
+    if (worst <= tol) { conv = true; break; }
+    if (precond == 1) {
+      // W <- (inexact) K^-1 W by the pipelined block PCG (FP32)
+      const size_t pblk = (size_t)c.max_rhs * vs;
+      double* b64 = c.pw64 + 6 * pblk;
+      float* d32 = c.pw32 + 9 * pblk;
+      int R = nb <= 1 ? 1 : nb <= 2 ? 2 : nb <= 4 ? 4 : 8;
+      cudaMemsetAsync(b64, 0, sizeof(double) * R * vs, s);
+      launch_convert(W, f64, b64, true, (long long)nb * vs, s);
+      if (pcg_pipe32(c, b64, d32, R, inner_rtol, inner_iters, nullptr, nullptr, nullptr, s)) return -2;
+      launch_convert(d32, false, W, f64, (long long)nb * vs, s);
+    }
+    const int ncols = it == 0 ? 2 * nb : 3 * nb;
+    if (launch_matvec(c, 0, f64, W, vec<T>(B.KS[cur], nb, vs), nb, nullptr, s)) return -2;
+    if (launch_matvec(c, 1, f64, W, vec<T>(B.MS[cur], nb, vs), nb, nullptr, s)) return -2;
+    launch_gram(c, f64, B.S[cur], ncols, B.KS[cur], ncols, GK, s);
+    launch_gram(c, f64, B.S[cur], ncols, B.MS[cur], ncols, GM, s);
+    lob_small_eig(c, ncols, nb, drop, s);
+    cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+    k_lob_update<T><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, ncols, vs, (T*)B.S[cur], (T*)B.KS[cur],
+                                                       (T*)B.MS[cur], C, (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1],
+                                                       (T*)B.MS[cur ^ 1]);
+    cur ^= 1;
+    (void)X;
+  }
+  if (iters_out) *iters_out = it;
+  // final FP64 Rayleigh-Ritz on fresh FP64 products
+  double* X6 = c.lw64;
+  double* KX6 = c.lw64 + (long long)c.max_modes * vs;
+  double* MX6 = c.lw64 + 2LL * c.max_modes * vs;
+  if (!f64) launch_convert(B.S[cur], false, X6, true, (long long)nb * vs, s);
+  else cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+  if (launch_matvec(c, 0, true, X6, KX6, nb, nullptr, s)) return -2;
+  if (launch_matvec(c, 1, true, X6, MX6, nb, nullptr, s)) return -2;
+  launch_gram(c, true, X6, nb, KX6, nb, GK, s);
+  launch_gram(c, true, X6, nb, MX6, nb, GM, s);
+  lob_small_eig(c, nb, nb, 1e-14, s);
+  // X64 = X6 C (first nmodes columns)
+  {
+    double* out = X64;
+    // reuse the update kernel: S = X6 (ncols = nb), P part unused -> KS2/MS2 scratch
+    double* scratch = c.lw64 + 3LL * c.max_modes * vs;   // FP64 LOBPCG area (free in mixed mode)
+    if (f64) scratch = (double*)B.S[cur ^ 1];
+    k_lob_update<double><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, nb, vs, X6, KX6, MX6, C, scratch,
+                                                            scratch + 3LL * c.max_modes * vs,
+                                                            scratch + 6LL * c.max_modes * vs);
+    cudaMemcpyAsync(out, scratch, sizeof(double) * nmodes * vs, cudaMemcpyDeviceToDevice, s);
+  }
+  cudaMemcpyAsync(hth, th, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
+  if (hinfo < 0) { c.last_error = "LOBPCG: final block rank deficient"; return -3; }
+  for (int j = 0; j < nmodes; ++j) lam[j] = hth[j];
+  return conv ? 0 : 1;
+}
+
+int lobpcg_run(Ctx& c, bool f64, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter,
+               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, int,
+               cudaStream_t s) {
+  if (f64)
+    return lobpcg_impl<double>(c, nmodes, nb, X64, lam, tol, maxiter, precond, inner_iters, inner_rtol, iters_out,
+                               resid_out, s);
+  return lobpcg_impl<float>(c, nmodes, nb, X64, lam, tol, maxiter, precond, inner_iters, inner_rtol, iters_out,
+                            resid_out, s);
+}
+
+}  // namespace tof
