@@ -45,11 +45,15 @@ enum {
 };
 enum { TOF_OP_K = 0, TOF_OP_M = 1 };
 enum { TOF_F32 = 0, TOF_F64 = 1 };
-/* TOF_MODE_FP64: plain FP64 Jacobi PCG / FP64 LOBPCG (the drop-in form).
- * TOF_MODE_MIXED: FP32 bulk arithmetic with FP64 iterative refinement (PCG)
- * or a final FP64 Rayleigh-Ritz (LOBPCG). */
-enum { TOF_MODE_FP64 = 0, TOF_MODE_MIXED = 1 };
-enum { TOF_PRECOND_JACOBI = 0, TOF_PRECOND_PCG = 1 };
+/* PCG modes.  TOF_MODE_FP64: plain FP64 Jacobi PCG, the reference's
+ * algorithm (the drop-in form).  TOF_MODE_MIXED: FP64 PCG preconditioned by
+ * an FP32 geometric-multigrid V-cycle (Galerkin coarse levels).
+ * TOF_MODE_IR: FP32 Jacobi PCG inside FP64 iterative refinement.
+ * LOBPCG: block vectors, Gram matrices and Rayleigh-Ritz are FP64 in every
+ * mode; TOF_MODE_FP64 uses the preconditioner requested, TOF_MODE_MIXED the
+ * FP32 multigrid V-cycle. */
+enum { TOF_MODE_FP64 = 0, TOF_MODE_MIXED = 1, TOF_MODE_IR = 2 };
+enum { TOF_PRECOND_JACOBI = 0, TOF_PRECOND_PCG = 1, TOF_PRECOND_MG = 2 };
 enum { TOF_FILTER_FORWARD = 0, TOF_FILTER_ADJOINT = 1, TOF_FILTER_PHYSICAL = 2 };
 enum {
   TOF_Q_NODES = 0, TOF_Q_ELEMS = 1, TOF_Q_FREE_DOFS = 2, TOF_Q_TILE_X = 3, TOF_Q_TILE_Y = 4,
@@ -122,6 +126,16 @@ int tof_diag(tof_ctx* ctx, int op, double* out, void* stream);
  * stats (host, nrhs entries) may be NULL. */
 int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double rtol, int maxiter,
             tof_solve_stats* stats, void* stream);
+
+/* Multigrid preconditioner introspection (no reference counterpart: the
+ * reference preconditions with diag(K) only).  tof_mg_query: number of
+ * levels (return value); for `level` >= 0 also its element dims (dims[3]) and
+ * the smoothing weight omega (host).  tof_mg_export: that level's Galerkin
+ * element matrices, FP32 [NE][576] (device; level >= 1).  tof_mg_apply: one
+ * V-cycle e = B r on R node4 FP32 vectors (R in 1, 2, 4, 8). */
+int tof_mg_query(tof_ctx* ctx, int level, int* dims, float* omega, void* stream);
+int tof_mg_export(tof_ctx* ctx, int level, float* out, void* stream);
+int tof_mg_apply(tof_ctx* ctx, const float* r, float* e, int R, void* stream);
 
 /* Lowest `nmodes` eigenpairs of K_ff x = lam M_ff x with a block of `block`
  * vectors (nmodes <= block <= 8).  X (device node4 FP64, `block` vectors)

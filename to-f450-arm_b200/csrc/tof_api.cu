@@ -106,6 +106,7 @@ static cudaError_t dalloc(Ctx& c, T** p, size_t n) {
 }
 
 static void free_ctx(Ctx& c) {
+  mg_destroy(c);
   void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
                   c.fK64, c.fM64, c.fK32, c.fM32, c.rho, c.dK64, c.dM64, c.dinvK64, c.dinvK32, c.partials,
                   c.bar, c.status, c.scal, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part};
@@ -225,6 +226,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.gram, 8 * 576));
   A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 576));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
+  if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error);
   A(cudaMemcpy(c.Ke64, Ke, 576 * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.Me64, Me, 576 * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.keb64, kb.data(), kb.size() * 8, cudaMemcpyHostToDevice));
@@ -280,6 +282,7 @@ int tof_set_density(tof_ctx* ctx, const double* rho, void* stream) {
   CUDA_TRY(cudaMemcpyAsync(c.rho, rho, sizeof(double) * c.g.NE, cudaMemcpyDeviceToDevice, s));
   launch_factors(c, c.rho, s);
   launch_diag(c, s);
+  mg_mark_dirty(c);
   CUDA_TRY(cudaGetLastError());
   return TOF_OK;
 }
@@ -395,8 +398,18 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       if (sk == ST_OK && rel[k] > rtol * 1.01) sk = ST_NOT_CONVERGED;
       st[k] = sk;
     }
+  } else if (mode == TOF_MODE_MIXED) {
+    // FP64 PCG preconditioned by the FP32 multigrid V-cycle
+    int ist[8] = {0};
+    if (pcg_mg64(c, wb, wx, R, rtol, maxiter, iters, ist, s)) return TOF_ERR_CUDA;
+    if (true_relres(c, wb, wx, R, rel, s)) return TOF_ERR_CUDA;
+    for (int k = 0; k < nrhs; ++k) {
+      outer[k] = 1;
+      st[k] = ist[k];
+      if (st[k] == ST_OK && rel[k] > rtol * 1.01) st[k] = ST_NOT_CONVERGED;
+    }
   } else {
-    // FP64 iterative refinement around the FP32 pipelined PCG
+    // FP64 iterative refinement around the FP32 standard PCG
     double* r64 = c.pw64 + 7 * blk;
     float* d32 = c.pw32 + 9 * blk;
     double bn[8], rn[8];
@@ -429,7 +442,8 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       if (all || o == max_outer || budget <= 0) break;
       // inner tolerance: a bit below what the worst rhs still needs
       const double inner = std::min(0.1, std::max(2e-5, 0.3 * need));
-      if (pcg_pipe32(c, r64, d32, R, inner, budget, nullptr, nullptr, nullptr, s)) return TOF_ERR_CUDA;
+      CUDA_TRY(cudaMemsetAsync(d32, 0, sizeof(float) * R * V, s));
+      if (pcg_std32(c, r64, d32, R, inner, budget, s)) return TOF_ERR_CUDA;
       int ist[16];
       CUDA_TRY(cudaMemcpyAsync(ist, c.status, sizeof(int) * 2 * R, cudaMemcpyDeviceToHost, s));
       launch_add_f32_to_f64((long long)R * V, d32, wx, s);
@@ -458,6 +472,24 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
     }
   }
   return rc;
+}
+
+int tof_mg_query(tof_ctx* ctx, int level, int* dims, float* omega, void* stream) {
+  if (!ctx) return TOF_ERR_ARG;
+  const int r = mg_query(ctx->c, level, dims, omega, (cudaStream_t)stream);
+  return r == -1 ? TOF_ERR_ARG : r == -2 ? TOF_ERR_CUDA : r;
+}
+
+int tof_mg_export(tof_ctx* ctx, int level, float* out, void* stream) {
+  if (!ctx || !out) return TOF_ERR_ARG;
+  const int r = mg_export(ctx->c, level, out, (cudaStream_t)stream);
+  return r == -1 ? TOF_ERR_ARG : r == -2 ? TOF_ERR_CUDA : TOF_OK;
+}
+
+int tof_mg_apply(tof_ctx* ctx, const float* r, float* e, int R, void* stream) {
+  if (!ctx || !r || !e) return TOF_ERR_ARG;
+  const int rc = mg_apply(ctx->c, r, e, R, (cudaStream_t)stream);
+  return rc == -1 ? TOF_ERR_ARG : rc == -2 ? TOF_ERR_CUDA : TOF_OK;
 }
 
 // ---------------------------------------------------------------------------

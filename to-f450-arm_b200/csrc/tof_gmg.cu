@@ -1,0 +1,1069 @@
+// Geometric multigrid on the structured voxel grid (sm_100a), FP32.
+//
+// The reference preconditions its Krylov solvers with diag(K) only
+// (src/fem.py:543-546, 441-443); on the SIMP-penalised arm that needs
+// ~1900 PCG iterations and ~2800 LOBPCG iterations.  This module provides a
+// V-cycle used as the preconditioner of an FP64 PCG (this file) and of the
+// FP64 LOBPCG (tof_lobpcg.cu):
+//
+// * hierarchy: each axis with >= 2 elements is coarsened 2:1 (ceil), axes of
+//   one element are kept (semi-coarsening), until the coarsest level has at
+//   most kCoarseNodes nodes;
+// * prolongation P: trilinear interpolation from coarse node I to fine node
+//   2I (+-1 with weight 1/2), with fixed fine DOFs masked out;
+// * coarse operators: Galerkin A_c = P^T A P, formed per coarse element as
+//   K_E = sum_children P_c^T (D_c f_c Ke D_c) P_c using the Kronecker
+//   structure P_c = W_c (x) I3 (8 x 8 scalar weights), so no matrix is
+//   assembled; levels >= 1 store one dense 24x24 FP32 matrix per element;
+// * smoother: damped Jacobi, nu pre- and nu post-sweeps (a symmetric V-cycle,
+//   hence an SPD preconditioner for CG); the fine-level sweeps use the
+//   TMA-tiled matrix-free stencil;
+// * coarsest level: dense FP64 inverse, built by one CTA (Cholesky, then
+//   L^-T L^-1), applied as a dense matvec.
+#include <math.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "tof_internal.h"
+#include "tof_stencil.cuh"
+
+namespace tof {
+
+constexpr int kCoarseNodes = 64;
+constexpr int kMaxLevels = 10;
+// Jacobi smoothing weight omega = kOmegaScale / lambda_max(D^-1 A).  4/3 is
+// the classical high-frequency-optimal choice; a 10-step power iteration
+// underestimates lambda_max by ~15 % on these operators, which keeps
+// omega * lambda_max near 1.6, inside the stable range (0, 2).
+constexpr float kOmegaScale = 1.3333f;
+constexpr int kPowerIters = 10;
+
+struct MGLevel {
+  int nx, ny, nz, NX, NY, NZ, NN, NE;
+  int fx, fy, fz;          // coarsening factor from the finer level (1 or 2)
+  float* Ae = nullptr;     // [NE][576] Galerkin element matrices (levels >= 1)
+  float* dinv = nullptr;   // node4
+  uint8_t* fix = nullptr;  // node bits
+  float *r = nullptr, *e = nullptr, *e2 = nullptr, *t = nullptr;   // node4 x maxR
+};
+
+struct MG {
+  int nlev = 0;
+  MGLevel L[kMaxLevels];
+  int nc = 0;                 // coarsest DOFs
+  double *A = nullptr, *Y = nullptr, *Ainv = nullptr;
+  int maxR = 0;
+  // damped-Jacobi weight per level, omega_l = kOmegaScale / lambda_l with
+  // lambda_l a power-iteration estimate of lambda_max(D^-1 A_l) (device)
+  float* omega = nullptr;
+  float* lam = nullptr;
+  int nu = 2;
+  bool dirty = true;
+  // outer FP64 PCG
+  double *x = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p[2] = {nullptr, nullptr};
+  double* S = nullptr;        // per-rhs scalars [8][8]
+  int* flags = nullptr;       // per-rhs frozen / status
+  unsigned* cnt = nullptr;    // last-block counters [8]
+  double* part = nullptr;     // partial sums
+  int part_blocks = 0;
+  int* info = nullptr;
+  // captured PCG iterations (kGraphIters per graph), one per R = 1, 2, 4, 8
+  cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool graph_failed = false;
+};
+constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void node_ijk(int n, int NX, int NY, int& i, int& j, int& k) {
+  i = n % NX; j = (n / NX) % NY; k = n / (NX * NY);
+}
+
+// Last-block-finishes reduction: every block adds its K partial sums; the last
+// block to arrive sums all partials in block order (deterministic) into
+// `total` and returns true.
+template <int K>
+__device__ bool last_block(double (&v)[K], double* part, unsigned* counter, double* scratch, double (&total)[K]) {
+  __shared__ int s_last;
+  block_sum<K>(v, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[(size_t)blockIdx.x * K + k] = v[k];
+    __threadfence();
+    const unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; ++k) total[k] = 0.0;
+  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) total[k] += __ldcg(part + (size_t)b * K + k);
+  }
+  block_sum<K>(total, scratch);
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin coarse element matrices
+// ---------------------------------------------------------------------------
+struct GalerkinArgs {
+  // fine level
+  int nx, ny, nz, NX, NY;
+  const float* Ae_f;       // fine element matrices (levels >= 1) or null
+  const double* fK;        // level-0 factors (when Ae_f is null)
+  const double* Ke;        // level-0 dense Ke
+  const uint8_t* fix0;     // level-0 node fixed bits
+  // coarse level
+  int cx, cy, cz;
+  int fx, fy, fz;
+  float* Ae_c;
+};
+
+__global__ void __launch_bounds__(128) k_mg_galerkin(GalerkinArgs a) {
+  __shared__ double Kc[576], T[576], W[64];
+  __shared__ double Dm[24];
+  __shared__ double fscale;
+  const int E = blockIdx.x;
+  const int ex = E % a.cx, ey = (E / a.cx) % a.cy, ez = E / (a.cx * a.cy);
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (int cd = 0; cd < a.fz; ++cd)
+    for (int cb = 0; cb < a.fy; ++cb)
+      for (int ca = 0; ca < a.fx; ++ca) {
+        const int fxe = a.fx * ex + ca, fye = a.fy * ey + cb, fze = a.fz * ez + cd;
+        if (fxe >= a.nx || fye >= a.ny || fze >= a.nz) continue;   // phantom child
+        const int ce = (fze * a.ny + fye) * a.nx + fxe;
+        if (threadIdx.x == 0) fscale = a.Ae_f ? 1.0 : a.fK[ce];
+        if (threadIdx.x < 24) {
+          double d = 1.0;
+          if (!a.Ae_f) {
+            const int l = threadIdx.x / 3, q = threadIdx.x % 3;
+            const int ox = (l == 1 || l == 2 || l == 5 || l == 6), oy = (l == 2 || l == 3 || l == 6 || l == 7),
+                      oz = l >= 4;
+            const int n = ((fze + oz) * a.NY + (fye + oy)) * a.NX + (fxe + ox);
+            d = ((a.fix0[n] >> q) & 1) ? 0.0 : 1.0;
+          }
+          Dm[threadIdx.x] = d;
+        }
+        if (threadIdx.x < 64) {
+          // weight of coarse corner m for child local node l
+          const int l = threadIdx.x / 8, m = threadIdx.x % 8;
+          const int ox = (l == 1 || l == 2 || l == 5 || l == 6), oy = (l == 2 || l == 3 || l == 6 || l == 7),
+                    oz = l >= 4;
+          const int mx = (m == 1 || m == 2 || m == 5 || m == 6), my = (m == 2 || m == 3 || m == 6 || m == 7),
+                    mz = m >= 4;
+          const double px = double(ca + ox) / a.fx, py = double(cb + oy) / a.fy, pz = double(cd + oz) / a.fz;
+          W[threadIdx.x] = (mx ? px : 1.0 - px) * (my ? py : 1.0 - py) * (mz ? pz : 1.0 - pz);
+        }
+        __syncthreads();
+        if (fscale == 0.0) { __syncthreads(); continue; }
+        for (int i = threadIdx.x; i < 576; i += blockDim.x) {
+          const int r = i / 24, c = i % 24;
+          Kc[i] = a.Ae_f ? double(a.Ae_f[(size_t)ce * 576 + i]) : fscale * a.Ke[i] * Dm[r] * Dm[c];
+        }
+        __syncthreads();
+        // T[i][3m+q] = sum_l Kc[i][3l+q] W[l][m]
+        for (int i = threadIdx.x; i < 576; i += blockDim.x) {
+          const int r = i / 24, col = i % 24, m = col / 3, q = col % 3;
+          double s = 0.0;
+#pragma unroll
+          for (int l = 0; l < 8; ++l) s = fma(Kc[r * 24 + 3 * l + q], W[l * 8 + m], s);
+          T[i] = s;
+        }
+        __syncthreads();
+        // acc[3m+q][col] += sum_l W[l][m] T[3l+q][col]
+        int slot = 0;
+        for (int i = threadIdx.x; i < 576; i += blockDim.x, ++slot) {
+          const int row = i / 24, col = i % 24, m = row / 3, q = row % 3;
+          double s = 0.0;
+#pragma unroll
+          for (int l = 0; l < 8; ++l) s = fma(W[l * 8 + m], T[(3 * l + q) * 24 + col], s);
+          acc[slot] += s;
+        }
+        __syncthreads();
+      }
+  int slot = 0;
+  for (int i = threadIdx.x; i < 576; i += blockDim.x, ++slot) a.Ae_c[(size_t)E * 576 + i] = float(acc[slot]);
+}
+
+// diag / inverse diag / fixed bits of a level >= 1 from its element matrices
+__global__ void k_mg_diag(int nx, int ny, int nz, const float* __restrict__ Ae, float* dinv, uint8_t* fix) {
+  const int NX = nx + 1, NY = ny + 1, NZ = nz + 1;
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= NX * NY * NZ) return;
+  int i, j, k;
+  node_ijk(n, NX, NY, i, j, k);
+  double d[3] = {0, 0, 0};
+  for (int c = -1; c <= 0; ++c)
+    for (int b = -1; b <= 0; ++b)
+      for (int a = -1; a <= 0; ++a) {
+        const int ex = i + a, ey = j + b, ez = k + c;
+        if (ex < 0 || ey < 0 || ez < 0 || ex >= nx || ey >= ny || ez >= nz) continue;
+        const int E = (ez * ny + ey) * nx + ex, ln = local_node(-a, -b, -c);
+        for (int q = 0; q < 3; ++q) d[q] += Ae[(size_t)E * 576 + (3 * ln + q) * 24 + 3 * ln + q];
+      }
+  uint8_t f = 0;
+  float4 o;
+  float* op = &o.x;
+  for (int q = 0; q < 3; ++q) {
+    const bool fz = !(d[q] > 0.0);
+    if (fz) f |= uint8_t(1u << q);
+    op[q] = fz ? 0.f : float(1.0 / d[q]);
+  }
+  o.w = 0.f;
+  reinterpret_cast<float4*>(dinv)[n] = o;
+  fix[n] = f;
+}
+
+// Coarsest level: dense assembly (row per thread), Cholesky, inverse.
+// Level 0 (Ae == null) assembles from factors and Ke with the fixed mask.
+__global__ void __launch_bounds__(256) k_mg_coarse_setup(int nx, int ny, int nz, const float* __restrict__ Ae,
+                                                         const double* __restrict__ fK, const double* __restrict__ Ke,
+                                                         const uint8_t* __restrict__ fix, double* A, double* Y,
+                                                         double* Ainv, int* info) {
+  const int NX = nx + 1, NY = ny + 1, NZ = nz + 1, NN = NX * NY * NZ, n = 3 * NN;
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) A[i] = 0.0;
+  __syncthreads();
+  for (int row = threadIdx.x; row < n; row += blockDim.x) {
+    const int N = row / 3, q = row % 3;
+    int i, j, k;
+    node_ijk(N, NX, NY, i, j, k);
+    const bool fixed_row = (fix[N] >> q) & 1;
+    for (int c = -1; c <= 0; ++c)
+      for (int b = -1; b <= 0; ++b)
+        for (int a = -1; a <= 0; ++a) {
+          const int ex = i + a, ey = j + b, ez = k + c;
+          if (ex < 0 || ey < 0 || ez < 0 || ex >= nx || ey >= ny || ez >= nz) continue;
+          const int E = (ez * ny + ey) * nx + ex, ln = local_node(-a, -b, -c);
+          for (int lm = 0; lm < 8; ++lm) {
+            const int mx = (lm == 1 || lm == 2 || lm == 5 || lm == 6), my = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
+                      mz = lm >= 4;
+            const int M = ((ez + mz) * NY + (ey + my)) * NX + (ex + mx);
+            for (int q2 = 0; q2 < 3; ++q2) {
+              const int col = 3 * M + q2;
+              const bool fixed_col = (fix[M] >> q2) & 1;
+              double v;
+              if (Ae) v = Ae[(size_t)E * 576 + (3 * ln + q) * 24 + 3 * lm + q2];
+              else v = fK[E] * Ke[(3 * ln + q) * 24 + 3 * lm + q2];
+              if (!fixed_row && !fixed_col) A[(size_t)row * n + col] += v;
+            }
+          }
+        }
+    if (fixed_row) A[(size_t)row * n + row] = 1.0;
+  }
+  __syncthreads();
+  // Cholesky (lower, in place)
+  __shared__ int s_bad;
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  for (int kk = 0; kk < n; ++kk) {
+    if (threadIdx.x == 0) {
+      const double d = A[(size_t)kk * n + kk];
+      if (!(d > 0.0)) { s_bad = kk + 1; A[(size_t)kk * n + kk] = 1.0; }
+      else A[(size_t)kk * n + kk] = sqrt(d);
+    }
+    __syncthreads();
+    const double piv = A[(size_t)kk * n + kk];
+    for (int i = kk + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + kk] /= piv;
+    __syncthreads();
+    const int m = n - kk - 1;
+    for (int w = threadIdx.x; w < m * m; w += blockDim.x) {
+      const int i = kk + 1 + w / m, j = kk + 1 + w % m;
+      if (j <= i) A[(size_t)i * n + j] -= A[(size_t)i * n + kk] * A[(size_t)j * n + kk];
+    }
+    __syncthreads();
+  }
+  // Y = L^-1 (column j by thread j)
+  for (int jc = threadIdx.x; jc < n; jc += blockDim.x) {
+    for (int i = 0; i < n; ++i) {
+      double s = (i == jc) ? 1.0 : 0.0;
+      for (int kk = jc; kk < i; ++kk) s -= A[(size_t)i * n + kk] * Y[(size_t)kk * n + jc];
+      Y[(size_t)i * n + jc] = i < jc ? 0.0 : s / A[(size_t)i * n + i];
+    }
+  }
+  __syncthreads();
+  // Ainv = Y^T Y, zero on fixed DOFs
+  for (int w = threadIdx.x; w < n * n; w += blockDim.x) {
+    const int i = w / n, j = w % n;
+    double s = 0.0;
+    for (int kk = max(i, j); kk < n; ++kk) s += Y[(size_t)kk * n + i] * Y[(size_t)kk * n + j];
+    const bool fi = (fix[i / 3] >> (i % 3)) & 1, fj = (fix[j / 3] >> (j % 3)) & 1;
+    Ainv[w] = (fi || fj) ? 0.0 : s;
+  }
+  if (threadIdx.x == 0) info[0] = s_bad;
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle kernels
+// ---------------------------------------------------------------------------
+struct LevelView {
+  int nx, ny, nz, NX, NY, NZ, NN;
+  const float* Ae;
+  const float* dinv;
+  const uint8_t* fix;
+};
+
+template <int R>
+__device__ __forceinline__ void elem_apply(const LevelView& L, int n, const float* __restrict__ x, long long vs,
+                                           float (&acc)[R][3]) {
+  int i, j, k;
+  node_ijk(n, L.NX, L.NY, i, j, k);
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
+  for (int c = -1; c <= 0; ++c)
+    for (int b = -1; b <= 0; ++b)
+      for (int a = -1; a <= 0; ++a) {
+        const int ex = i + a, ey = j + b, ez = k + c;
+        if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
+        const int E = (ez * L.ny + ey) * L.nx + ex, ln = local_node(-a, -b, -c);
+        const float* Kr = L.Ae + (size_t)E * 576 + (3 * ln) * 24;
+#pragma unroll
+        for (int lm = 0; lm < 8; ++lm) {
+          const int mx = (lm == 1 || lm == 2 || lm == 5 || lm == 6), my = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
+                    mz = lm >= 4;
+          const int M = ((ez + mz) * L.NY + (ey + my)) * L.NX + (ex + mx);
+          float k0[3], k1[3], k2[3];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            k0[q] = __ldg(Kr + 3 * lm + q);
+            k1[q] = __ldg(Kr + 24 + 3 * lm + q);
+            k2[q] = __ldg(Kr + 48 + 3 * lm + q);
+          }
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const float4 xv = __ldg(reinterpret_cast<const float4*>(x + r * vs) + M);
+            acc[r][0] += k0[0] * xv.x + k0[1] * xv.y + k0[2] * xv.z;
+            acc[r][1] += k1[0] * xv.x + k1[1] * xv.y + k1[2] * xv.z;
+            acc[r][2] += k2[0] * xv.x + k2[1] * xv.y + k2[2] * xv.z;
+          }
+        }
+      }
+}
+
+// mode 0: y = b - A x;  mode 1: y = x + omega D^-1 (b - A x);  mode 2: y = D^-1 A x
+template <int R>
+__global__ void __launch_bounds__(128) k_mgc_op(LevelView L, const float* __restrict__ x, const float* __restrict__ b,
+                                                float* y, const float* __restrict__ omega_p, int mode) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= L.NN) return;
+  const long long vs = (long long)L.NN * 4;
+  float acc[R][3];
+  elem_apply<R>(L, n, x, vs, acc);
+  const uint8_t fx = L.fix[n];
+  const float4 di = reinterpret_cast<const float4*>(L.dinv)[n];
+  const float omega = mode == 1 ? __ldg(omega_p) : 0.f;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (mode == 2) {
+      reinterpret_cast<float4*>(y + r * vs)[n] =
+          make_float4(di.x * acc[r][0], di.y * acc[r][1], di.z * acc[r][2], 0.f);
+      continue;
+    }
+    const float4 bb = reinterpret_cast<const float4*>(b + r * vs)[n];
+    float4 o = make_float4(bb.x - acc[r][0], bb.y - acc[r][1], bb.z - acc[r][2], 0.f);
+    if (mode == 1) {
+      const float4 xc = reinterpret_cast<const float4*>(x + r * vs)[n];
+      o.x = fmaf(omega * di.x, o.x, xc.x);
+      o.y = fmaf(omega * di.y, o.y, xc.y);
+      o.z = fmaf(omega * di.z, o.z, xc.z);
+    }
+    o.x = (fx & 1) ? 0.f : o.x;
+    o.y = (fx & 2) ? 0.f : o.y;
+    o.z = (fx & 4) ? 0.f : o.z;
+    reinterpret_cast<float4*>(y + r * vs)[n] = o;
+  }
+}
+
+// e = omega D^-1 r  (first pre-smoothing sweep from e = 0), any level
+__global__ void k_mg_jacobi0(int NN, int R, const float* __restrict__ dinv, const float* __restrict__ r, float* e,
+                             const float* __restrict__ omega_p) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)NN * R) return;
+  const int n = int(idx % NN);
+  const float omega = __ldg(omega_p);
+  const float4 d = reinterpret_cast<const float4*>(dinv)[n];
+  const float4 v = reinterpret_cast<const float4*>(r)[idx];
+  reinterpret_cast<float4*>(e)[idx] = make_float4(omega * d.x * v.x, omega * d.y * v.y, omega * d.z * v.z, 0.f);
+}
+
+// power iteration for lambda_max(D^-1 A): start vector, D^-1 scaling, estimate
+__global__ void k_mg_power_init(int NN, const uint8_t* __restrict__ fix, float* x) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= NN) return;
+  float v[3];
+  for (int q = 0; q < 3; ++q) {
+    unsigned h = (unsigned)(n * 3 + q) * 2654435761u;   // multiplicative hash
+    h ^= h >> 15; h *= 2246822519u; h ^= h >> 13;
+    v[q] = ((fix[n] >> q) & 1) ? 0.f : float(h & 0xffff) / 32768.f - 1.f;
+  }
+  reinterpret_cast<float4*>(x)[n] = make_float4(v[0], v[1], v[2], 0.f);
+}
+
+__global__ void k_mg_scale_dinv(int NN, const float* __restrict__ dinv, float* y) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= NN) return;
+  const float4 d = reinterpret_cast<const float4*>(dinv)[n];
+  float4 v = reinterpret_cast<float4*>(y)[n];
+  v.x *= d.x; v.y *= d.y; v.z *= d.z;
+  reinterpret_cast<float4*>(y)[n] = v;
+}
+
+// lambda = ||x_k|| / ||x_{k-1}||, omega = scale / lambda (one CTA)
+__global__ void __launch_bounds__(1024) k_mg_lambda(int NN, const float* __restrict__ xp, const float* __restrict__ xl,
+                                                    float* lam, float* omega, float scale) {
+  __shared__ double red[2 * 32];
+  double v[2] = {0.0, 0.0};
+  for (int n = threadIdx.x; n < NN; n += blockDim.x) {
+    const float4 a = reinterpret_cast<const float4*>(xp)[n];
+    const float4 b = reinterpret_cast<const float4*>(xl)[n];
+    v[0] += double(a.x) * a.x + double(a.y) * a.y + double(a.z) * a.z;
+    v[1] += double(b.x) * b.x + double(b.y) * b.y + double(b.z) * b.z;
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    const double l = (v[0] > 0.0 && v[1] > 0.0) ? sqrt(v[1] / v[0]) : 4.0;
+    *lam = float(l);
+    *omega = float(scale / fmax(l, 1e-3));
+  }
+}
+
+struct Transfer {
+  int NXf, NYf, NZf;   // fine nodes
+  int NXc, NYc, NZc;   // coarse nodes
+  int fx, fy, fz;
+};
+
+// r_c = P^T t_f (masked by the coarse fixed bits)
+template <int R>
+__global__ void k_mg_restrict(Transfer T, const float* __restrict__ tf, const uint8_t* __restrict__ fixc, float* rc) {
+  const int N = blockIdx.x * blockDim.x + threadIdx.x;
+  const int NNc = T.NXc * T.NYc * T.NZc;
+  if (N >= NNc) return;
+  int I, J, K;
+  node_ijk(N, T.NXc, T.NYc, I, J, K);
+  const long long vsf = (long long)T.NXf * T.NYf * T.NZf * 4, vsc = (long long)NNc * 4;
+  float acc[R][3];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
+  const int dz0 = T.fz == 2 ? -1 : 0, dz1 = T.fz == 2 ? 1 : 0;
+  const int dy0 = T.fy == 2 ? -1 : 0, dy1 = T.fy == 2 ? 1 : 0;
+  const int dx0 = T.fx == 2 ? -1 : 0, dx1 = T.fx == 2 ? 1 : 0;
+  for (int dk = dz0; dk <= dz1; ++dk) {
+    const int k = T.fz * K + dk;
+    if (k < 0 || k >= T.NZf) continue;
+    for (int dj = dy0; dj <= dy1; ++dj) {
+      const int j = T.fy * J + dj;
+      if (j < 0 || j >= T.NYf) continue;
+      for (int di = dx0; di <= dx1; ++di) {
+        const int i = T.fx * I + di;
+        if (i < 0 || i >= T.NXf) continue;
+        const float w = (dk ? 0.5f : 1.f) * (dj ? 0.5f : 1.f) * (di ? 0.5f : 1.f);
+        const int n = (k * T.NYf + j) * T.NXf + i;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(tf + r * vsf) + n);
+          acc[r][0] += w * v.x; acc[r][1] += w * v.y; acc[r][2] += w * v.z;
+        }
+      }
+    }
+  }
+  const uint8_t fx = fixc[N];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    reinterpret_cast<float4*>(rc + r * vsc)[N] = make_float4((fx & 1) ? 0.f : acc[r][0], (fx & 2) ? 0.f : acc[r][1],
+                                                             (fx & 4) ? 0.f : acc[r][2], 0.f);
+}
+
+// e_f += P e_c (masked by the fine fixed bits)
+template <int R>
+__global__ void k_mg_prolong(Transfer T, const float* __restrict__ ec, const uint8_t* __restrict__ fixf, float* ef) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  const int NNf = T.NXf * T.NYf * T.NZf;
+  if (n >= NNf) return;
+  int i, j, k;
+  node_ijk(n, T.NXf, T.NYf, i, j, k);
+  const long long vsf = (long long)NNf * 4, vsc = (long long)T.NXc * T.NYc * T.NZc * 4;
+  int Ix[2], Iy[2], Iz[2];
+  float wx[2], wy[2], wz[2];
+  int cx, cy, cz;
+  auto axis = [](int f, int i_, int* I_, float* w_, int& c_) {
+    if (f == 1 || (i_ & 1) == 0) { I_[0] = f == 1 ? i_ : i_ / 2; w_[0] = 1.f; c_ = 1; }
+    else { I_[0] = (i_ - 1) / 2; I_[1] = (i_ + 1) / 2; w_[0] = w_[1] = 0.5f; c_ = 2; }
+  };
+  axis(T.fx, i, Ix, wx, cx);
+  axis(T.fy, j, Iy, wy, cy);
+  axis(T.fz, k, Iz, wz, cz);
+  float acc[R][3];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
+  for (int c = 0; c < cz; ++c)
+    for (int b = 0; b < cy; ++b)
+      for (int a = 0; a < cx; ++a) {
+        const float w = wx[a] * wy[b] * wz[c];
+        const int N = (Iz[c] * T.NYc + Iy[b]) * T.NXc + Ix[a];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float4 v = __ldg(reinterpret_cast<const float4*>(ec + r * vsc) + N);
+          acc[r][0] += w * v.x; acc[r][1] += w * v.y; acc[r][2] += w * v.z;
+        }
+      }
+  const uint8_t fx = fixf[n];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    float4 o = reinterpret_cast<float4*>(ef + r * vsf)[n];
+    if (!(fx & 1)) o.x += acc[r][0];
+    if (!(fx & 2)) o.y += acc[r][1];
+    if (!(fx & 4)) o.z += acc[r][2];
+    reinterpret_cast<float4*>(ef + r * vsf)[n] = o;
+  }
+}
+
+// coarsest: e = Ainv r (one CTA, n <= 3 * kCoarseNodes)
+__global__ void __launch_bounds__(256) k_mg_coarse_solve(int NN, int R, const double* __restrict__ Ainv,
+                                                         const float* __restrict__ r, float* e) {
+  __shared__ double sr[8][3 * kCoarseNodes];
+  const int n = 3 * NN;
+  for (int w = threadIdx.x; w < R * n; w += blockDim.x) {
+    const int rr = w / n, i = w % n;
+    sr[rr][i] = double(r[(size_t)rr * NN * 4 + (i / 3) * 4 + i % 3]);
+  }
+  __syncthreads();
+  for (int w = threadIdx.x; w < R * n; w += blockDim.x) {
+    const int rr = w / n, i = w % n;
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s = fma(Ainv[(size_t)i * n + j], sr[rr][j], s);
+    e[(size_t)rr * NN * 4 + (i / 3) * 4 + i % 3] = float(s);
+  }
+  for (int w = threadIdx.x; w < R * NN; w += blockDim.x) e[(size_t)(w / NN) * NN * 4 + (w % NN) * 4 + 3] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// host: hierarchy, setup, V-cycle
+// ---------------------------------------------------------------------------
+static LevelView view(const MGLevel& L) {
+  return LevelView{L.nx, L.ny, L.nz, L.NX, L.NY, L.NZ, L.NN, L.Ae, L.dinv, L.fix};
+}
+static Transfer transfer(const MGLevel& f, const MGLevel& c) {
+  return Transfer{f.NX, f.NY, f.NZ, c.NX, c.NY, c.NZ, c.fx, c.fy, c.fz};
+}
+
+int mg_create(Ctx& c, int maxR) {
+  MG* mg = new MG();
+  c.mg = mg;
+  mg->maxR = maxR;
+  int nx = c.g.nx, ny = c.g.ny, nz = c.g.nz;
+  int l = 0;
+  while (true) {
+    MGLevel& L = mg->L[l];
+    L.nx = nx; L.ny = ny; L.nz = nz;
+    L.NX = nx + 1; L.NY = ny + 1; L.NZ = nz + 1;
+    L.NN = L.NX * L.NY * L.NZ;
+    L.NE = nx * ny * nz;
+    if (l == 0) { L.fx = L.fy = L.fz = 1; }
+    const bool can = nx >= 2 || ny >= 2 || nz >= 2;
+    if (L.NN <= kCoarseNodes || !can || l == kMaxLevels - 1) { mg->nlev = l + 1; break; }
+    MGLevel& C = mg->L[l + 1];
+    C.fx = nx >= 2 ? 2 : 1; C.fy = ny >= 2 ? 2 : 1; C.fz = nz >= 2 ? 2 : 1;
+    nx = (nx + C.fx - 1) / C.fx; ny = (ny + C.fy - 1) / C.fy; nz = (nz + C.fz - 1) / C.fz;
+    ++l;
+  }
+  const MGLevel& last = mg->L[mg->nlev - 1];
+  if (last.NN > kCoarseNodes) { c.last_error = "multigrid: coarsest level too large"; return -1; }
+  mg->nc = 3 * last.NN;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  auto al = [&](auto** p, size_t n) {
+    using T = std::remove_pointer_t<std::remove_reference_t<decltype(*p)>>;
+    const size_t b = std::max<size_t>(n, 1) * sizeof(T);
+    c.bytes += b;
+    A(cudaMalloc((void**)p, b));
+    A(cudaMemset(*p, 0, b));
+  };
+  for (int k = 0; k < mg->nlev; ++k) {
+    MGLevel& L = mg->L[k];
+    const size_t V = (size_t)L.NN * 4 * maxR;
+    if (k > 0) {
+      al(&L.Ae, (size_t)L.NE * 576);
+      al(&L.dinv, (size_t)L.NN * 4);
+      al(&L.fix, (size_t)L.NN);
+    } else {
+      L.dinv = c.dinvK32;
+      L.fix = c.fix;
+    }
+    al(&L.r, V); al(&L.e, V); al(&L.e2, V); al(&L.t, V);
+  }
+  const size_t n2 = (size_t)mg->nc * mg->nc;
+  al(&mg->A, n2); al(&mg->Y, n2); al(&mg->Ainv, n2);
+  const size_t V0 = (size_t)c.g.NN * 4 * maxR;
+  al(&mg->x, V0); al(&mg->r, V0); al(&mg->z, V0); al(&mg->q, V0); al(&mg->p[0], V0); al(&mg->p[1], V0);
+  al(&mg->S, 256); al(&mg->flags, 64); al(&mg->cnt, 16); al(&mg->info, 16);
+  al(&mg->omega, kMaxLevels); al(&mg->lam, kMaxLevels);
+  mg->part_blocks = std::max(c.g.ntiles, 4 * c.num_sms);
+  al(&mg->part, (size_t)mg->part_blocks * 3 * 8);
+  if (e != cudaSuccess) { c.last_error = std::string("multigrid alloc: ") + cudaGetErrorString(e); return -2; }
+  return 0;
+}
+
+void mg_destroy(Ctx& c) {
+  MG* mg = c.mg;
+  if (!mg) return;
+  for (int k = 0; k < mg->nlev; ++k) {
+    MGLevel& L = mg->L[k];
+    if (k > 0) { cudaFree(L.Ae); cudaFree(L.dinv); cudaFree(L.fix); }
+    cudaFree(L.r); cudaFree(L.e); cudaFree(L.e2); cudaFree(L.t);
+  }
+  for (auto& g : mg->gexec)
+    if (g) cudaGraphExecDestroy(g);
+  void* ps[] = {mg->A, mg->Y, mg->Ainv, mg->x, mg->r, mg->z, mg->q, mg->p[0], mg->p[1], mg->S, mg->flags, mg->cnt,
+                mg->info, mg->part, mg->omega, mg->lam};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  delete mg;
+  c.mg = nullptr;
+}
+
+// Rebuild coarse operators after a density change.
+int mg_setup(Ctx& c, cudaStream_t s) {
+  MG* mg = c.mg;
+  for (int k = 1; k < mg->nlev; ++k) {
+    MGLevel& F = mg->L[k - 1];
+    MGLevel& C = mg->L[k];
+    GalerkinArgs a;
+    a.nx = F.nx; a.ny = F.ny; a.nz = F.nz; a.NX = F.NX; a.NY = F.NY;
+    a.Ae_f = k == 1 ? nullptr : F.Ae;
+    a.fK = c.fK64; a.Ke = c.Ke64; a.fix0 = c.fix;
+    a.cx = C.nx; a.cy = C.ny; a.cz = C.nz;
+    a.fx = C.fx; a.fy = C.fy; a.fz = C.fz;
+    a.Ae_c = C.Ae;
+    k_mg_galerkin<<<C.NE, 128, 0, s>>>(a);
+    k_mg_diag<<<ceil_div(C.NN, 128), 128, 0, s>>>(C.nx, C.ny, C.nz, C.Ae, C.dinv, C.fix);
+  }
+  const MGLevel& L = mg->L[mg->nlev - 1];
+  k_mg_coarse_setup<<<1, 256, 0, s>>>(L.nx, L.ny, L.nz, mg->nlev > 1 ? L.Ae : nullptr, c.fK64, c.Ke64, L.fix, mg->A,
+                                      mg->Y, mg->Ainv, mg->info);
+  // smoothing weights: power iteration on D^-1 A_l (scratch: the level's e, e2)
+  for (int k = 0; k < mg->nlev - 1; ++k) {
+    MGLevel& V = mg->L[k];
+    float* x = V.e;
+    float* y = V.e2;
+    k_mg_power_init<<<ceil_div(V.NN, 256), 256, 0, s>>>(V.NN, V.fix, x);
+    for (int it = 0; it < kPowerIters; ++it) {
+      if (k == 0) {
+        if (launch_matvec(c, 0, false, x, y, 1, nullptr, s)) return -2;
+        k_mg_scale_dinv<<<ceil_div(V.NN, 256), 256, 0, s>>>(V.NN, V.dinv, y);
+      } else {
+        k_mgc_op<1><<<ceil_div(V.NN, 128), 128, 0, s>>>(view(V), x, nullptr, y, nullptr, 2);
+      }
+      std::swap(x, y);
+    }
+    k_mg_lambda<<<1, 1024, 0, s>>>(V.NN, y, x, mg->lam + k, mg->omega + k, kOmegaScale);
+  }
+  mg->dirty = false;
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+template <int R>
+static int vcycle_t(Ctx& c, cudaStream_t s) {
+  MG* mg = c.mg;
+  const int nl = mg->nlev;
+  auto grid1 = [](int n) { return ceil_div(n, 128); };
+  // Jacobi sweeps ping-pong between e and e2; the first sweep writes to
+  // whichever buffer makes the last sweep of the level land in L.e, so the
+  // buffer roles are the same in every V-cycle (required for graph replay).
+  float* cur[kMaxLevels];
+  float* alt[kMaxLevels];
+  for (int k = 0; k < nl; ++k) {
+    const bool odd = ((2 * mg->nu - 1) & 1) != 0;   // sweeps after the first
+    cur[k] = odd ? mg->L[k].e2 : mg->L[k].e;
+    alt[k] = odd ? mg->L[k].e : mg->L[k].e2;
+  }
+  // downward
+  for (int k = 0; k < nl - 1; ++k) {
+    MGLevel& L = mg->L[k];
+    const float* om = mg->omega + k;
+    k_mg_jacobi0<<<ceil_div(L.NN * R, 256), 256, 0, s>>>(L.NN, R, L.dinv, L.r, cur[k], om);
+    for (int sw = 1; sw < mg->nu; ++sw) {
+      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
+      else k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1);
+      std::swap(cur[k], alt[k]);
+    }
+    if (k == 0) { if (launch_matvec(c, 0, false, cur[k], L.t, R, L.r, s)) return -2; }
+    else k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, L.t, nullptr, 0);
+    MGLevel& C = mg->L[k + 1];
+    k_mg_restrict<R><<<grid1(C.NN), 128, 0, s>>>(transfer(L, C), L.t, C.fix, C.r);
+  }
+  {
+    MGLevel& L = mg->L[nl - 1];
+    k_mg_coarse_solve<<<1, 256, 0, s>>>(L.NN, R, mg->Ainv, L.r, L.e);
+    cur[nl - 1] = L.e;
+  }
+  // upward
+  for (int k = nl - 2; k >= 0; --k) {
+    MGLevel& L = mg->L[k];
+    MGLevel& C = mg->L[k + 1];
+    k_mg_prolong<R><<<grid1(L.NN), 128, 0, s>>>(transfer(L, C), cur[k + 1], L.fix, cur[k]);
+    const float* om = mg->omega + k;
+    for (int sw = 0; sw < mg->nu; ++sw) {
+      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
+      else k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1);
+      std::swap(cur[k], alt[k]);
+    }
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// Apply the V-cycle to mg->L[0].r (R vectors); result in mg->L[0].e.
+int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
+  if (c.mg->nlev == 1) {
+    MGLevel& L = c.mg->L[0];
+    k_mg_coarse_solve<<<1, 256, 0, s>>>(L.NN, R, c.mg->Ainv, L.r, L.e);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+  }
+  switch (R) {
+    case 1: return vcycle_t<1>(c, s);
+    case 2: return vcycle_t<2>(c, s);
+    case 4: return vcycle_t<4>(c, s);
+    case 8: return vcycle_t<8>(c, s);
+  }
+  return -1;
+}
+
+int mg_query(Ctx& c, int level, int* dims, float* omega, cudaStream_t s) {
+  MG* mg = c.mg;
+  if (level < 0) return mg->nlev;
+  if (level >= mg->nlev) return -1;
+  if (mg->dirty && mg_setup(c, s)) return -2;
+  if (dims) { dims[0] = mg->L[level].nx; dims[1] = mg->L[level].ny; dims[2] = mg->L[level].nz; }
+  if (omega) {
+    if (level < mg->nlev - 1) {
+      cudaMemcpyAsync(omega, mg->omega + level, sizeof(float), cudaMemcpyDeviceToHost, s);
+      cudaStreamSynchronize(s);
+    } else {
+      *omega = 0.f;
+    }
+  }
+  return mg->nlev;
+}
+
+int mg_export(Ctx& c, int level, float* out, cudaStream_t s) {
+  MG* mg = c.mg;
+  if (level < 1 || level >= mg->nlev) return -1;
+  if (mg->dirty && mg_setup(c, s)) return -2;
+  const MGLevel& L = mg->L[level];
+  return cudaMemcpyAsync(out, L.Ae, sizeof(float) * 576 * (size_t)L.NE, cudaMemcpyDeviceToDevice, s) == cudaSuccess
+             ? 0
+             : -2;
+}
+
+int mg_apply(Ctx& c, const float* r, float* e, int R, cudaStream_t s) {
+  MG* mg = c.mg;
+  if (R != 1 && R != 2 && R != 4 && R != 8) return -1;
+  if (R > mg->maxR) return -1;
+  if (mg->dirty && mg_setup(c, s)) return -2;
+  const size_t bytes = sizeof(float) * 4 * (size_t)c.g.NN * R;
+  cudaMemcpyAsync(mg->L[0].r, r, bytes, cudaMemcpyDeviceToDevice, s);
+  if (mg_vcycle(c, R, s)) return -2;
+  return cudaMemcpyAsync(e, mg->L[0].e, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -2;
+}
+
+void mg_mark_dirty(Ctx& c) {
+  if (c.mg) c.mg->dirty = true;
+}
+int mg_ensure(Ctx& c, cudaStream_t s) { return c.mg->dirty ? mg_setup(c, s) : 0; }
+float* mg_rhs(Ctx& c) { return c.mg->L[0].r; }
+float* mg_out(Ctx& c) { return c.mg->L[0].e; }
+int mg_levels(const Ctx& c) { return c.mg ? c.mg->nlev : 0; }
+
+// ---------------------------------------------------------------------------
+// FP64 PCG preconditioned by the FP32 V-cycle
+// ---------------------------------------------------------------------------
+// scalar layout per rhs k: S[k*8 + {0: rz, 1: alpha, 2: beta, 3: rr, 4: bnorm, 5: iters}]
+// flags[k]: 0 active, 1 converged, 2 breakdown / non-finite
+
+// r = b - A x0 already computed into mg->r; r32 = (float) r; rr, bb
+template <int R>
+__global__ void __launch_bounds__(256) k_mgpcg_init(int NN, const double* __restrict__ b, const double* __restrict__ r,
+                                                   float* r32, double* p0, double* S, int* flags, double* part,
+                                                   unsigned* cnt, double rtol) {
+  __shared__ double red[2 * R * 32];
+  double v[2 * R];
+#pragma unroll
+  for (int k = 0; k < 2 * R; ++k) v[k] = 0.0;
+  const long long vs = (long long)NN * 4;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const double4 rr = reinterpret_cast<const double4*>(r + k * vs)[n];
+      const double4 bb = reinterpret_cast<const double4*>(b + k * vs)[n];
+      reinterpret_cast<float4*>(r32 + k * vs)[n] = make_float4(float(rr.x), float(rr.y), float(rr.z), 0.f);
+      reinterpret_cast<double4*>(p0 + k * vs)[n] = make_double4(0, 0, 0, 0);
+      v[2 * k] += rr.x * rr.x + rr.y * rr.y + rr.z * rr.z;
+      v[2 * k + 1] += bb.x * bb.x + bb.y * bb.y + bb.z * bb.z;
+    }
+  }
+  double tot[2 * R];
+  if (last_block<2 * R>(v, part, cnt, red, tot) && threadIdx.x == 0) {
+    for (int k = 0; k < R; ++k) {
+      const double bn = sqrt(tot[2 * k + 1]);
+      S[k * 8 + 3] = tot[2 * k];
+      S[k * 8 + 4] = bn;
+      S[k * 8 + 6] = rtol;
+      S[k * 8 + 5] = 0.0;
+      S[k * 8 + 2] = 0.0;
+      int f = 0;
+      if (!isfinite(tot[2 * k]) || !isfinite(bn)) f = 2;
+      else if (!(bn > 0.0) || sqrt(tot[2 * k]) <= rtol * bn) f = 1;
+      flags[k] = f;
+    }
+  }
+}
+
+// z = (double) e0; rz = r.z; beta = rz / rz_prev (first: 0)
+template <int R>
+__global__ void __launch_bounds__(256) k_mgpcg_zrz(int NN, const float* __restrict__ e0, const double* __restrict__ r,
+                                                  double* z, double* S, const int* flags, double* part, unsigned* cnt,
+                                                  int first) {
+  __shared__ double red[R * 32];
+  double v[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = 0.0;
+  const long long vs = (long long)NN * 4;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const float4 e = reinterpret_cast<const float4*>(e0 + k * vs)[n];
+      const double4 rr = reinterpret_cast<const double4*>(r + k * vs)[n];
+      reinterpret_cast<double4*>(z + k * vs)[n] = make_double4(e.x, e.y, e.z, 0.0);
+      v[k] += rr.x * e.x + rr.y * e.y + rr.z * e.z;
+    }
+  }
+  double tot[R];
+  if (last_block<R>(v, part, cnt, red, tot) && threadIdx.x == 0) {
+    for (int k = 0; k < R; ++k) {
+      if (flags[k]) continue;
+      const double rz = tot[k];
+      S[k * 8 + 2] = first ? 0.0 : rz / S[k * 8 + 0];
+      S[k * 8 + 0] = rz;
+    }
+  }
+}
+
+// p_new = z + beta p_old; q = A p_new; alpha = rz / p.q (tile kernel, FP64)
+template <int R>
+__global__ void __launch_bounds__(256) k_mgpcg_pq(const __grid_constant__ CUtensorMap tmz,
+                                                 const __grid_constant__ CUtensorMap tmp, Grid g,
+                                                 const double* __restrict__ fK, const double* __restrict__ keb,
+                                                 const uint8_t* __restrict__ fix, double* pn, double* q, double* S,
+                                                 int* flags, double* part, unsigned* cnt) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  using V4 = double4;
+  const TileGeom tg = tile_geom(g, blockIdx.x);
+  const unsigned hbytes = halo_bytes<double>(g, R);
+  double* sz = reinterpret_cast<double*>(smem);
+  double* sp = reinterpret_cast<double*>(smem + hbytes);
+  double* sKe = reinterpret_cast<double*>(smem + 2 * hbytes);
+  double* sf = sKe + kKeBlocksLen;
+  const int nfe = tg.EX * tg.EY * tg.EZ;
+  double* red = sf + nfe;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(red + R * 32);
+  __shared__ double beta[R];
+  __shared__ int fz[R];
+  if (threadIdx.x == 0) {
+    mbar_init(mbar, 1);
+    mbar_arrive_expect_tx(mbar, 2 * hbytes);
+    tma_load_5d(sz, &tmz, 0, tg.i0 - 1, tg.j0 - 1, tg.k0 - 1, 0, mbar);
+    tma_load_5d(sp, &tmp, 0, tg.i0 - 1, tg.j0 - 1, tg.k0 - 1, 0, mbar);
+  }
+  if (threadIdx.x < R) { beta[threadIdx.x] = S[threadIdx.x * 8 + 2]; fz[threadIdx.x] = flags[threadIdx.x]; }
+  load_ke_blocks(keb, sKe);
+  load_factor_tile(g, tg, fK, sf);
+  __syncthreads();   // mbarrier initialised before anyone waits on it
+  const bool ok = __syncthreads_and(mbar_wait(mbar, 0));
+  const int hsr = tg.HX * tg.HY * tg.HZ;
+  if (ok) {
+    for (int idx = threadIdx.x; idx < R * hsr; idx += blockDim.x) {
+      const int k = idx / hsr;
+      const V4 z4 = reinterpret_cast<V4*>(sz)[idx];
+      V4 p4 = reinterpret_cast<V4*>(sp)[idx];
+      const double be = fz[k] ? 0.0 : beta[k];
+      p4.x = fma(be, p4.x, z4.x); p4.y = fma(be, p4.y, z4.y); p4.z = fma(be, p4.z, z4.z); p4.w = 0.0;
+      reinterpret_cast<V4*>(sp)[idx] = p4;
+    }
+  }
+  __syncthreads();
+  double v[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = 0.0;
+  int tx, ty, tz, n;
+  if (ok && thread_node(g, tg, tx, ty, tz, n)) {
+    double acc[R][3];
+    stencil_node<double, R>(sp, tg, sf, sKe, tx, ty, tz, acc);
+    const uint8_t fx = __ldg(fix + n);
+    const long long vs = (long long)g.NN * 4;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const V4 pp = halo_center<double>(sp, tg, k, tx, ty, tz);
+      const V4 qq = make_double4((fx & 1) ? 0.0 : acc[k][0], (fx & 2) ? 0.0 : acc[k][1], (fx & 4) ? 0.0 : acc[k][2], 0.0);
+      reinterpret_cast<V4*>(q + k * vs)[n] = qq;
+      reinterpret_cast<V4*>(pn + k * vs)[n] = pp;
+      v[k] += pp.x * qq.x + pp.y * qq.y + pp.z * qq.z;
+    }
+  }
+  double tot[R];
+  if (last_block<R>(v, part, cnt, red, tot) && threadIdx.x == 0) {
+    for (int k = 0; k < R; ++k) {
+      if (flags[k]) { S[k * 8 + 1] = 0.0; continue; }
+      if (!isfinite(tot[k]) || !(tot[k] > 0.0)) { flags[k] = 2; S[k * 8 + 1] = 0.0; continue; }
+      S[k * 8 + 1] = S[k * 8 + 0] / tot[k];
+    }
+  }
+  if (!ok && threadIdx.x == 0) atomicExch(flags + 8, ST_TIMEOUT);
+}
+
+// x += alpha p; r -= alpha q; r32 = (float) r; rr; convergence flags
+template <int R>
+__global__ void __launch_bounds__(256) k_mgpcg_xr(int NN, const double* __restrict__ p, const double* __restrict__ q,
+                                                 double* x, double* r, float* r32, double* S, int* flags,
+                                                 double* part, unsigned* cnt) {
+  __shared__ double red[R * 32];
+  __shared__ double al[R];
+  __shared__ int fz[R];
+  if (threadIdx.x < R) { al[threadIdx.x] = S[threadIdx.x * 8 + 1]; fz[threadIdx.x] = flags[threadIdx.x]; }
+  __syncthreads();
+  double v[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = 0.0;
+  const long long vs = (long long)NN * 4;
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const size_t o = k * vs / 4 + n;
+      double4 rr = reinterpret_cast<const double4*>(r)[o];
+      if (!fz[k]) {
+        const double a = al[k];
+        const double4 pp = reinterpret_cast<const double4*>(p)[o];
+        const double4 qq = reinterpret_cast<const double4*>(q)[o];
+        double4 xx = reinterpret_cast<const double4*>(x)[o];
+        xx.x = fma(a, pp.x, xx.x); xx.y = fma(a, pp.y, xx.y); xx.z = fma(a, pp.z, xx.z);
+        rr.x = fma(-a, qq.x, rr.x); rr.y = fma(-a, qq.y, rr.y); rr.z = fma(-a, qq.z, rr.z);
+        reinterpret_cast<double4*>(x)[o] = xx;
+        reinterpret_cast<double4*>(r)[o] = rr;
+      }
+      reinterpret_cast<float4*>(r32)[o] = make_float4(float(rr.x), float(rr.y), float(rr.z), 0.f);
+      v[k] += rr.x * rr.x + rr.y * rr.y + rr.z * rr.z;
+    }
+  }
+  double tot[R];
+  if (last_block<R>(v, part, cnt, red, tot) && threadIdx.x == 0) {
+    for (int k = 0; k < R; ++k) {
+      if (flags[k]) continue;
+      S[k * 8 + 3] = tot[k];
+      S[k * 8 + 5] += 1.0;
+      if (!isfinite(tot[k])) flags[k] = 2;
+      else if (sqrt(tot[k]) <= S[k * 8 + 6] * S[k * 8 + 4]) flags[k] = 1;
+    }
+  }
+}
+
+template <int R>
+static int mgpcg_iter(Ctx& c, int pc, cudaStream_t s) {
+  MG* mg = c.mg;
+  const int eb = std::min(ceil_div(c.g.NN, 256), 2 * c.num_sms);
+  std::string err;
+  CUtensorMap tmz, tmp;
+  if (!encode_node4_map(&tmz, mg->z, c.g, R, true, &err) || !encode_node4_map(&tmp, mg->p[pc], c.g, R, true, &err)) {
+    c.last_error = err;
+    return -2;
+  }
+  const int nfe = (c.g.TX + 1) * (c.g.TY + 1) * (c.g.TZ + 1);
+  const size_t smem = 2 * size_t(halo_bytes<double>(c.g, R)) + 8 * (kKeBlocksLen + nfe) + 8 * R * 32 + 16;
+  auto kern = k_mgpcg_pq<R>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<c.g.ntiles, c.g.TX * c.g.TY * c.g.TZ, smem, s>>>(tmz, tmp, c.g, c.fK64, c.keb64, c.fix, mg->p[pc ^ 1], mg->q,
+                                                           mg->S, mg->flags, mg->part, mg->cnt + 0);
+  k_mgpcg_xr<R><<<eb, 256, 0, s>>>(c.g.NN, mg->p[pc ^ 1], mg->q, mg->x, mg->r, mg->L[0].r, mg->S, mg->flags, mg->part,
+                                   mg->cnt + 1);
+  if (mg_vcycle(c, R, s)) return -2;
+  k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->L[0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 0);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// Solve K x = b (R node4 FP64 rhs, x holds x0 and the result) to rtol.
+template <int R>
+static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter, int* iters, int* status,
+                   cudaStream_t s) {
+  MG* mg = c.mg;
+  const size_t V = (size_t)c.g.NN * 4;
+  if (mg->dirty && mg_setup(c, s)) return -2;
+  cudaMemsetAsync(mg->flags, 0, sizeof(int) * 16, s);
+  cudaMemsetAsync(mg->cnt, 0, sizeof(unsigned) * 16, s);
+  cudaMemcpyAsync(mg->x, x, sizeof(double) * R * V, cudaMemcpyDeviceToDevice, s);
+  if (launch_matvec(c, 0, true, mg->x, mg->r, R, b, s)) return -2;
+  const int eb = std::min(ceil_div(c.g.NN, 256), 2 * c.num_sms);
+  k_mgpcg_init<R><<<eb, 256, 0, s>>>(c.g.NN, b, mg->r, mg->L[0].r, mg->p[0], mg->S, mg->flags, mg->part, mg->cnt + 3,
+                                     rtol);
+  if (mg_vcycle(c, R, s)) return -2;
+  k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->L[0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 1);
+  int it = 0;
+  int hf[9];
+  const int ri = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : 3;
+  while (true) {
+    cudaMemcpyAsync(hf, mg->flags, sizeof(int) * 9, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "multigrid PCG: CUDA error"; return -2; }
+    bool all = true;
+    for (int k = 0; k < R; ++k) all = all && hf[k] != 0;
+    if (all || it >= maxiter || hf[8]) break;
+    // kGraphIters iterations per step: a replay of the captured graph when
+    // the stream can be captured, else eager launches (same kernels)
+    if (!mg->gexec[ri] && !mg->graph_failed) {
+      cudaGraph_t graph = nullptr;
+      bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      for (int q = 0; ok && q < kGraphIters; ++q) ok = mgpcg_iter<R>(c, q & 1, s) == 0;
+      const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
+      if (ok && ended && graph && cudaGraphInstantiate(&mg->gexec[ri], graph, 0) == cudaSuccess) {
+        // captured
+      } else {
+        mg->gexec[ri] = nullptr;
+        mg->graph_failed = true;
+      }
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
+    }
+    if (mg->gexec[ri]) {
+      if (cudaGraphLaunch(mg->gexec[ri], s) != cudaSuccess) { c.last_error = "multigrid PCG: graph launch"; return -2; }
+    } else {
+      for (int q = 0; q < kGraphIters; ++q)
+        if (mgpcg_iter<R>(c, q & 1, s)) return -2;
+    }
+    it += kGraphIters;
+  }
+  cudaMemcpyAsync(x, mg->x, sizeof(double) * R * V, cudaMemcpyDeviceToDevice, s);
+  double hs[64];
+  cudaMemcpyAsync(hs, mg->S, sizeof(double) * 8 * R, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "multigrid PCG: CUDA error"; return -2; }
+  for (int k = 0; k < R; ++k) {
+    iters[k] = int(hs[k * 8 + 5]);
+    status[k] = hf[8] ? ST_TIMEOUT : hf[k] == 1 ? ST_OK : hf[k] == 2 ? ST_BREAKDOWN : ST_NOT_CONVERGED;
+  }
+  return 0;
+}
+
+int pcg_mg64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int* iters, int* status,
+             cudaStream_t s) {
+  switch (R) {
+    case 1: return mgpcg_t<1>(c, b, x, rtol, maxiter, iters, status, s);
+    case 2: return mgpcg_t<2>(c, b, x, rtol, maxiter, iters, status, s);
+    case 4: return mgpcg_t<4>(c, b, x, rtol, maxiter, iters, status, s);
+    case 8: return mgpcg_t<8>(c, b, x, rtol, maxiter, iters, status, s);
+  }
+  c.last_error = "multigrid PCG: nrhs must be 1, 2, 4 or 8";
+  return -1;
+}
+
+}  // namespace tof

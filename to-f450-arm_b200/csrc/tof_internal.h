@@ -12,6 +12,8 @@
 
 namespace tof {
 
+struct MG;
+
 struct SimpParams {
   double penal = 3.0;          // SIMP exponent p (src/fem.py:204)
   double emin = 1e-9;          // E_min / E (src/fem.py:205)
@@ -70,6 +72,7 @@ struct Ctx {
   int coop_plain[9] = {0};
 
 
+  MG* mg = nullptr;                // multigrid hierarchy (tof_gmg.cu)
   std::vector<uint8_t> host_fix;   // host copy of `fix`
   size_t bytes = 0;
   std::string last_error;
@@ -83,6 +86,8 @@ void launch_factors(Ctx& c, const double* rho, cudaStream_t s);
 void launch_diag(Ctx& c, cudaStream_t s);
 int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, const void* b_residual,
                   cudaStream_t s);
+int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* omega, int R,
+                   cudaStream_t s);
 void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s);
 void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s);
 void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s);
@@ -96,5 +101,23 @@ int pcg_plain64(Ctx& c, const double* b, double* x, int R, double rtol, int maxi
                 int* status, cudaStream_t s);
 int pcg_pipe32(Ctx& c, const double* b, float* d, int R, double rtol, int maxiter, int* iters, double* relres,
                int* status, cudaStream_t s);
+// FP32 standard PCG from x = 0 (x must be zeroed by the caller)
+int pcg_std32(Ctx& c, const double* b, float* x, int R, double rtol, int maxiter, cudaStream_t s);
+
+// multigrid (tof_gmg.cu)
+int mg_create(Ctx& c, int maxR);
+void mg_destroy(Ctx& c);
+int mg_setup(Ctx& c, cudaStream_t s);
+void mg_mark_dirty(Ctx& c);
+int mg_ensure(Ctx& c, cudaStream_t s);
+int mg_vcycle(Ctx& c, int R, cudaStream_t s);   // mg_rhs -> mg_out
+float* mg_rhs(Ctx& c);
+float* mg_out(Ctx& c);
+int mg_levels(const Ctx& c);
+int mg_query(Ctx& c, int level, int* dims, float* omega, cudaStream_t s);
+int mg_export(Ctx& c, int level, float* out, cudaStream_t s);
+int mg_apply(Ctx& c, const float* r, float* e, int R, cudaStream_t s);
+int pcg_mg64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int* iters, int* status,
+             cudaStream_t s);
 
 }  // namespace tof

@@ -92,6 +92,8 @@ struct MatvecArgs {
   const T* b;          // residual mode: rhs, else null
   T* y;
   long long vstride;   // elements between consecutive vectors (NN*4)
+  const T* dinv;       // smoother mode (with b): y = x + omega D^-1 (b - A x)
+  const float* omega;  // device scalar (smoother mode)
 };
 
 template <typename T, int R>
@@ -132,6 +134,14 @@ __global__ void __launch_bounds__(512) k_matvec(const __grid_constant__ CUtensor
     if (a.b) {
       const V4 bb = reinterpret_cast<const V4*>(a.b + r * a.vstride)[n];
       out.x = bb.x - acc[r][0]; out.y = bb.y - acc[r][1]; out.z = bb.z - acc[r][2];
+      if (a.dinv) {
+        const V4 xc = halo_center<T>(sx, tg, r, tx, ty, tz);
+        const V4 di = reinterpret_cast<const V4*>(a.dinv)[n];
+        const T om = T(__ldg(a.omega));
+        out.x = fma(om * di.x, out.x, xc.x);
+        out.y = fma(om * di.y, out.y, xc.y);
+        out.z = fma(om * di.z, out.z, xc.z);
+      }
     } else {
       out.x = acc[r][0]; out.y = acc[r][1]; out.z = acc[r][2];
     }
@@ -144,7 +154,8 @@ __global__ void __launch_bounds__(512) k_matvec(const __grid_constant__ CUtensor
 }
 
 template <typename T, int R>
-static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b, cudaStream_t s) {
+static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b, cudaStream_t s,
+                           const void* dinv = nullptr, const float* omega = nullptr) {
   CUtensorMap tm;
   std::string err;
   if (!encode_node4_map(&tm, x, c.g, R, sizeof(T) == 8, &err)) {
@@ -163,6 +174,8 @@ static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b
   a.b = reinterpret_cast<const T*>(b);
   a.y = reinterpret_cast<T*>(y);
   a.vstride = (long long)c.g.NN * 4;
+  a.dinv = reinterpret_cast<const T*>(dinv);
+  a.omega = omega;
   const TileGeom tg{0, 0, 0, c.g.TX + 2, c.g.TY + 2, c.g.TZ + 2, c.g.TX + 1, c.g.TY + 1, c.g.TZ + 1};
   size_t smem = halo_bytes<T>(c.g, R) + sizeof(T) * (kKeBlocksLen + tg.EX * tg.EY * tg.EZ);
   smem = ((smem + 15) & ~size_t(15)) + 16;
@@ -203,6 +216,17 @@ int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, co
     done += R;
   }
   return 0;
+}
+
+// y = x + omega D^-1 (b - K x) on the fine level, FP32, R in {1,2,4,8}
+int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* omega, int R,
+                   cudaStream_t s) {
+  switch (R) {
+    case 8: return matvec_launch_t<float, 8>(c, 0, x, y, b, s, dinv, omega);
+    case 4: return matvec_launch_t<float, 4>(c, 0, x, y, b, s, dinv, omega);
+    case 2: return matvec_launch_t<float, 2>(c, 0, x, y, b, s, dinv, omega);
+    default: return matvec_launch_t<float, 1>(c, 0, x, y, b, s, dinv, omega);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -296,18 +296,20 @@ __global__ void __launch_bounds__(256) k_pcg_pipe(const __grid_constant__ PipeAr
 }
 
 // ===========================================================================
-// FP64 plain PCG (the reference's recurrence)
+// Standard (SciPy-recurrence) Jacobi PCG, vectors in T = double (the plain
+// FP64 drop-in) or T = float (the inner solver of FP64 refinement); scalars,
+// dot products and the rhs are FP64 either way.
 // ===========================================================================
-template <int R>
+template <typename T, int R>
 struct PlainArgs {
   CUtensorMap tmx, tmz, tmp[2];
   Grid g;
-  const double* fK;
-  const double* keb;
+  const T* fK;
+  const T* keb;
   const uint8_t* fix;
-  const double* dinv;
+  const T* dinv;
   const double* b;
-  double *x, *r, *z, *q, *p[2];
+  T *x, *r, *z, *q, *p[2];
   double* partials;
   BarrierState* bar;
   int* status;
@@ -317,18 +319,25 @@ struct PlainArgs {
   long long vs;
 };
 
-template <int R>
-__global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ PlainArgs<R> a) {
+template <typename V4, typename S>
+__device__ __forceinline__ V4 v4(S x, S y, S z) {
+  V4 o;
+  o.x = x; o.y = y; o.z = z; o.w = 0;
+  return o;
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ PlainArgs<T, R> a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  using V4 = double4;
+  using V4 = typename Vec4<T>::type;
   const Grid& g = a.g;
-  const unsigned hbytes = halo_bytes<double>(g, R);
-  double* sz = reinterpret_cast<double*>(smem);
-  double* sp = reinterpret_cast<double*>(smem + hbytes);
-  double* sKe = reinterpret_cast<double*>(smem + 2 * hbytes);
-  double* sf = sKe + kKeBlocksLen;
+  const unsigned hbytes = halo_bytes<T>(g, R);
+  T* sz = reinterpret_cast<T*>(smem);
+  T* sp = reinterpret_cast<T*>(smem + hbytes);
+  T* sKe = reinterpret_cast<T*>(smem + 2 * hbytes);
+  T* sf = sKe + kKeBlocksLen;
   const int nfe = (g.TX + 1) * (g.TY + 1) * (g.TZ + 1);
-  double* red = sf + nfe;
+  double* red = reinterpret_cast<double*>(smem + ((2 * hbytes + sizeof(T) * (kKeBlocksLen + nfe) + 15) & ~15u));
   uint64_t* mbar = reinterpret_cast<uint64_t*>(red + 3 * R * 32);
   __shared__ SolveShared st;
 
@@ -358,25 +367,23 @@ __global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ Plain
       phase ^= 1;
       int tx, ty, tz, n;
       if (ok && thread_node(g, tg, tx, ty, tz, n)) {
-        double acc[R][3];
-        stencil_node<double, R>(sp, tg, sf, sKe, tx, ty, tz, acc);
+        T acc[R][3];
+        stencil_node<T, R>(sp, tg, sf, sKe, tx, ty, tz, acc);
         const uint8_t fx = __ldg(a.fix + n);
         const V4 di = reinterpret_cast<const V4*>(a.dinv)[n];
 #pragma unroll
         for (int k = 0; k < R; ++k) {
           const size_t o = k * a.vs / 4 + n;
-          const V4 bb = reinterpret_cast<const V4*>(a.b)[o];
-          V4 rr;
-          rr.x = (fx & 1) ? 0.0 : bb.x - acc[k][0];
-          rr.y = (fx & 2) ? 0.0 : bb.y - acc[k][1];
-          rr.z = (fx & 4) ? 0.0 : bb.z - acc[k][2];
-          rr.w = 0.0;
-          const V4 zz = make_double4(di.x * rr.x, di.y * rr.y, di.z * rr.z, 0.0);
+          const double4 bb = reinterpret_cast<const double4*>(a.b)[o];
+          const V4 rr = v4<V4, T>((fx & 1) ? T(0) : T(bb.x - double(acc[k][0])),
+                                  (fx & 2) ? T(0) : T(bb.y - double(acc[k][1])),
+                                  (fx & 4) ? T(0) : T(bb.z - double(acc[k][2])));
+          const V4 zz = v4<V4, T>(di.x * rr.x, di.y * rr.y, di.z * rr.z);
           reinterpret_cast<V4*>(a.r)[o] = rr;
           reinterpret_cast<V4*>(a.z)[o] = zz;
-          reinterpret_cast<V4*>(a.p[0])[o] = make_double4(0, 0, 0, 0);
-          v[3 * k + 0] += rr.x * zz.x + rr.y * zz.y + rr.z * zz.z;
-          v[3 * k + 1] += rr.x * rr.x + rr.y * rr.y + rr.z * rr.z;
+          reinterpret_cast<V4*>(a.p[0])[o] = v4<V4, T>(T(0), T(0), T(0));
+          v[3 * k + 0] += double(rr.x) * zz.x + double(rr.y) * zz.y + double(rr.z) * zz.z;
+          v[3 * k + 1] += double(rr.x) * rr.x + double(rr.y) * rr.y + double(rr.z) * rr.z;
           const double bx = (fx & 1) ? 0.0 : bb.x, by = (fx & 2) ? 0.0 : bb.y, bz = (fx & 4) ? 0.0 : bb.z;
           v[3 * k + 2] += bx * bx + by * by + bz * bz;
         }
@@ -439,31 +446,28 @@ __global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ Plain
       for (int idx = threadIdx.x; idx < R * hsr; idx += blockDim.x) {
         const int k = idx / hsr;
         if (st.frozen[k]) continue;
-        const double be = st.beta[k];
+        const T be = T(st.beta[k]);
         V4 pz = reinterpret_cast<V4*>(sz)[idx];
         V4 pp = reinterpret_cast<V4*>(sp)[idx];
-        pp.x = fma(be, pp.x, pz.x); pp.y = fma(be, pp.y, pz.y); pp.z = fma(be, pp.z, pz.z); pp.w = 0.0;
+        pp.x = fma(be, pp.x, pz.x); pp.y = fma(be, pp.y, pz.y); pp.z = fma(be, pp.z, pz.z); pp.w = T(0);
         reinterpret_cast<V4*>(sp)[idx] = pp;
       }
       __syncthreads();
       int tx, ty, tz, n;
       if (ok && thread_node(g, tg, tx, ty, tz, n)) {
-        double acc[R][3];
-        stencil_node<double, R>(sp, tg, sf, sKe, tx, ty, tz, acc);
+        T acc[R][3];
+        stencil_node<T, R>(sp, tg, sf, sKe, tx, ty, tz, acc);
         const uint8_t fx = __ldg(a.fix + n);
 #pragma unroll
         for (int k = 0; k < R; ++k) {
           if (st.frozen[k]) continue;
           const size_t o = k * a.vs / 4 + n;
-          const V4 pp = halo_center<double>(sp, tg, k, tx, ty, tz);
-          V4 qq;
-          qq.x = (fx & 1) ? 0.0 : acc[k][0];
-          qq.y = (fx & 2) ? 0.0 : acc[k][1];
-          qq.z = (fx & 4) ? 0.0 : acc[k][2];
-          qq.w = 0.0;
+          const V4 pp = halo_center<T>(sp, tg, k, tx, ty, tz);
+          const V4 qq = v4<V4, T>((fx & 1) ? T(0) : acc[k][0], (fx & 2) ? T(0) : acc[k][1],
+                                  (fx & 4) ? T(0) : acc[k][2]);
           reinterpret_cast<V4*>(a.q)[o] = qq;
           reinterpret_cast<V4*>(a.p[pn])[o] = pp;
-          v[k] += pp.x * qq.x + pp.y * qq.y + pp.z * qq.z;
+          v[k] += double(pp.x) * qq.x + double(pp.y) * qq.y + double(pp.z) * qq.z;
         }
       }
       __syncthreads();
@@ -497,19 +501,19 @@ __global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ Plain
       for (int k = 0; k < R; ++k) {
         if (st.frozen[k]) continue;
         const size_t o = k * a.vs / 4 + n;
-        const double al = st.alpha[k];
+        const T al = T(st.alpha[k]);
         const V4 pp = reinterpret_cast<const V4*>(a.p[pn])[o];
         const V4 qq = reinterpret_cast<const V4*>(a.q)[o];
         V4 xx = reinterpret_cast<const V4*>(a.x)[o];
         V4 rr = reinterpret_cast<const V4*>(a.r)[o];
         xx.x = fma(al, pp.x, xx.x); xx.y = fma(al, pp.y, xx.y); xx.z = fma(al, pp.z, xx.z);
         rr.x = fma(-al, qq.x, rr.x); rr.y = fma(-al, qq.y, rr.y); rr.z = fma(-al, qq.z, rr.z);
-        const V4 zz = make_double4(di.x * rr.x, di.y * rr.y, di.z * rr.z, 0.0);
+        const V4 zz = v4<V4, T>(di.x * rr.x, di.y * rr.y, di.z * rr.z);
         reinterpret_cast<V4*>(a.x)[o] = xx;
         reinterpret_cast<V4*>(a.r)[o] = rr;
         reinterpret_cast<V4*>(a.z)[o] = zz;
-        w[2 * k] += rr.x * zz.x + rr.y * zz.y + rr.z * zz.z;
-        w[2 * k + 1] += rr.x * rr.x + rr.y * rr.y + rr.z * rr.z;
+        w[2 * k] += double(rr.x) * zz.x + double(rr.y) * zz.y + double(rr.z) * zz.z;
+        w[2 * k + 1] += double(rr.x) * rr.x + double(rr.y) * rr.y + double(rr.z) * rr.z;
       }
     }
     write_partials<2 * R>(a.partials, w, red);
@@ -554,9 +558,12 @@ static size_t pipe_smem(const Grid& g, int R) {
   s += sizeof(double) * 3 * R * 32 + 16;
   return s;
 }
+template <typename T>
 static size_t plain_smem(const Grid& g, int R) {
   const int nfe = (g.TX + 1) * (g.TY + 1) * (g.TZ + 1);
-  return 2 * size_t(halo_bytes<double>(g, R)) + 8 * (kKeBlocksLen + nfe) + sizeof(double) * 3 * R * 32 + 16;
+  size_t s = 2 * size_t(halo_bytes<T>(g, R)) + sizeof(T) * (kKeBlocksLen + nfe);
+  s = (s + 15) & ~size_t(15);
+  return s + sizeof(double) * 3 * R * 32 + 16;
 }
 
 template <int R>
@@ -591,22 +598,29 @@ static int pipe_launch(Ctx& c, const double* b, float* d, double rtol, int maxit
   return 0;
 }
 
-template <int R>
-static int plain_launch(Ctx& c, const double* b, double* x, double rtol, int maxiter, cudaStream_t s) {
-  PlainArgs<R> a;
+template <typename T, int R>
+static int plain_launch(Ctx& c, const double* b, T* x, double rtol, int maxiter, cudaStream_t s) {
+  constexpr bool f64 = sizeof(T) == 8;
+  PlainArgs<T, R> a;
   a.g = c.g;
-  a.fK = c.fK64; a.keb = c.keb64; a.fix = c.fix; a.dinv = c.dinvK64; a.b = b;
+  if constexpr (f64) {
+    a.fK = c.fK64; a.keb = c.keb64; a.dinv = c.dinvK64;
+  } else {
+    a.fK = c.fK32; a.keb = c.keb32; a.dinv = c.dinvK32;
+  }
+  a.fix = c.fix; a.b = b;
   const size_t blk = (size_t)c.max_rhs * c.g.NN * 4;
-  double* w = c.pw64;
+  T* w;
+  if constexpr (f64) w = c.pw64; else w = c.pw32 + blk;   // FP32: slots 2..6
   a.x = x; a.r = w + blk; a.z = w + 2 * blk; a.q = w + 3 * blk; a.p[0] = w + 4 * blk; a.p[1] = w + 5 * blk;
   a.partials = c.partials; a.bar = c.bar; a.status = c.status; a.relres = c.scal;
   a.rtol = rtol; a.maxiter = maxiter; a.vs = (long long)c.g.NN * 4;
   std::string err;
-  if (!encode_node4_map(&a.tmx, a.x, c.g, R, true, &err) || !encode_node4_map(&a.tmz, a.z, c.g, R, true, &err) ||
-      !encode_node4_map(&a.tmp[0], a.p[0], c.g, R, true, &err) ||
-      !encode_node4_map(&a.tmp[1], a.p[1], c.g, R, true, &err)) { c.last_error = err; return -2; }
-  const size_t smem = plain_smem(c.g, R);
-  auto kern = k_pcg_plain<R>;
+  if (!encode_node4_map(&a.tmx, a.x, c.g, R, f64, &err) || !encode_node4_map(&a.tmz, a.z, c.g, R, f64, &err) ||
+      !encode_node4_map(&a.tmp[0], a.p[0], c.g, R, f64, &err) ||
+      !encode_node4_map(&a.tmp[1], a.p[1], c.g, R, f64, &err)) { c.last_error = err; return -2; }
+  const size_t smem = plain_smem<T>(c.g, R);
+  auto kern = k_pcg_plain<T, R>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, c.g.TX * c.g.TY * c.g.TZ, smem);
@@ -625,12 +639,23 @@ static int plain_launch(Ctx& c, const double* b, double* x, double rtol, int max
 int pcg_plain64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int*, double*, int*,
                 cudaStream_t s) {
   switch (R) {
-    case 1: return plain_launch<1>(c, b, x, rtol, maxiter, s);
-    case 2: return plain_launch<2>(c, b, x, rtol, maxiter, s);
-    case 4: return plain_launch<4>(c, b, x, rtol, maxiter, s);
-    case 8: return plain_launch<8>(c, b, x, rtol, maxiter, s);
+    case 1: return plain_launch<double, 1>(c, b, x, rtol, maxiter, s);
+    case 2: return plain_launch<double, 2>(c, b, x, rtol, maxiter, s);
+    case 4: return plain_launch<double, 4>(c, b, x, rtol, maxiter, s);
+    case 8: return plain_launch<double, 8>(c, b, x, rtol, maxiter, s);
   }
   c.last_error = "plain PCG: nrhs must be 1, 2, 4 or 8";
+  return -1;
+}
+
+int pcg_std32(Ctx& c, const double* b, float* x, int R, double rtol, int maxiter, cudaStream_t s) {
+  switch (R) {
+    case 1: return plain_launch<float, 1>(c, b, x, rtol, maxiter, s);
+    case 2: return plain_launch<float, 2>(c, b, x, rtol, maxiter, s);
+    case 4: return plain_launch<float, 4>(c, b, x, rtol, maxiter, s);
+    case 8: return plain_launch<float, 8>(c, b, x, rtol, maxiter, s);
+  }
+  c.last_error = "FP32 PCG: nrhs must be 1, 2, 4 or 8";
   return -1;
 }
 

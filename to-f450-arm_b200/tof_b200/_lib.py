@@ -15,8 +15,8 @@ TOF_OK, TOF_NOT_CONVERGED = 0, 1
 TOF_ERR_ARG, TOF_ERR_CUDA, TOF_ERR_BREAKDOWN, TOF_ERR_NONFINITE, TOF_ERR_TIMEOUT = -1, -2, -3, -4, -5
 OP_K, OP_M = 0, 1
 F32, F64 = 0, 1
-MODE_FP64, MODE_MIXED = 0, 1
-PRECOND_JACOBI, PRECOND_PCG = 0, 1
+MODE_FP64, MODE_MIXED, MODE_IR = 0, 1, 2
+PRECOND_JACOBI, PRECOND_PCG, PRECOND_MG = 0, 1, 2
 FILTER_FORWARD, FILTER_ADJOINT, FILTER_PHYSICAL = 0, 1, 2
 Q_NODES, Q_ELEMS, Q_FREE_DOFS, Q_TILE_X, Q_TILE_Y, Q_TILE_Z, Q_DEVICE_BYTES, Q_MAX_RHS, Q_MAX_MODES = range(9)
 
@@ -69,6 +69,9 @@ SIGNATURES = {
     "tof_filter_apply": (c_int, [P, c_int, P, P, P]),
     "tof_filter_destroy": (None, [P]),
     "tof_oc_update": (c_int, [c_int, P, P, c_double, c_double, c_double, P, P, P]),
+    "tof_mg_query": (c_int, [P, c_int, POINTER(c_int), POINTER(ctypes.c_float), P]),
+    "tof_mg_export": (c_int, [P, c_int, P, P]),
+    "tof_mg_apply": (c_int, [P, P, P, c_int, P]),
 }
 
 _lib = None

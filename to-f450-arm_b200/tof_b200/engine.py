@@ -182,6 +182,31 @@ class DesignContext:
                                                       float(lam), float(vMv_tip), L.ptr(out), _stream()), self.h)
         return out
 
+    # -- multigrid introspection ------------------------------------------ #
+    def mg_levels(self):
+        """[(nx, ny, nz, omega)] per multigrid level (omega 0 on the coarsest)."""
+        n = self.lib.tof_mg_query(self.h, -1, None, None, _stream())
+        out = []
+        for lv in range(n):
+            dims = (c_int * 3)()
+            om = ctypes.c_float()
+            L.check("tof_mg_query", min(0, self.lib.tof_mg_query(self.h, lv, dims, ctypes.byref(om), _stream())),
+                    self.h)
+            out.append((dims[0], dims[1], dims[2], om.value))
+        return out
+
+    def mg_element_matrices(self, level: int) -> torch.Tensor:
+        nx, ny, nz, _ = self.mg_levels()[level]
+        out = torch.empty((nx * ny * nz, 24, 24), dtype=torch.float32, device=self.device)
+        L.check("tof_mg_export", self.lib.tof_mg_export(self.h, level, L.ptr(out), _stream()), self.h)
+        return out
+
+    def mg_apply(self, r4: torch.Tensor) -> torch.Tensor:
+        r4 = r4.to(torch.float32).contiguous()
+        e = torch.empty_like(r4)
+        L.check("tof_mg_apply", self.lib.tof_mg_apply(self.h, L.ptr(r4), L.ptr(e), r4.shape[0], _stream()), self.h)
+        return e
+
     def effective_mass(self, modes4: torch.Tensor, direction=2) -> np.ndarray:
         m = modes4.to(torch.float64).contiguous()
         out = (c_double * m.shape[0])()
