@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""SIMP design iterations per second on one B200 (per GPU replica).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one full SIMP design iteration on the 2 mm arm grid (110 x 14 x 12
+voxels, 64 935 DOF): density filter, four load cases solved as one block
+(FP64 PCG preconditioned by an FP32 multigrid V-cycle, relative residual
+1e-8), six lowest modes (FP64 LOBPCG with the FP32 multigrid preconditioner,
+eigenvalues converged to ~1e-10), MAC tracking, eigenvalue and compliance
+sensitivities, the augmented-Lagrangian frequency penalty and the OC update.
+Inputs are synthetic (seeded) with the shapes of the reference's arm; see
+tof_b200/workloads.py.  With N GPUs every rank runs an independent replica
+(the path does not shard); value = N * K / max-rank time.
+
+Also reported: the same iteration in the plain FP64 form (Jacobi PCG per load
+case, Jacobi LOBPCG: the reference's algorithms), seconds per PCG / LOBPCG
+solve in both forms on the hollow-box arm with their errors against the
+reference's FP64 results (tests/golden/arm.npz), the dominant kernel's
+roofline, and the reference algorithm timed on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "to-f450-arm_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "SIMP iter/s"
+WORKLOAD = ("arm 110x14x12 @2mm, one SIMP design iteration: 4 load cases (block PCG, rel. residual 1e-8) "
+            "+ 6 modes (LOBPCG, eigenvalues to ~1e-10) + adjoint sensitivities + filter r=1.5 + OC, vf 0.08")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="own", choices=["own", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip FP64/solver/CPU comparisons")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- #
+def reference_arm(a, rank, world):
+    """The reference's algorithm on the host cores (oracle port), bounded."""
+    if rank != 0:
+        return
+    from oracle.cpu_bench import simp_iteration_sample
+    from tof_b200 import configs as C
+    geom = C.arm_geometry()
+    rho = C.arm_hollow_density(geom)
+    F = C.arm_static_loads(geom)
+    F = F + [F[0]]
+    times = []
+    info = None
+    for s in range(a.warmup + a.steps):
+        info = simp_iteration_sample(geom, C.PA12.E, C.PA12.nu, C.PA12.rho, rho, F, C.TIP_MASS_KG,
+                                     geom.motor_mount_top_nodes(), n_modes=6, lob_iters=25,
+                                     design_mask=geom.build_masks()["design"])
+        if s >= a.warmup:
+            times.append(info["t_iter_s"])
+    t = float(np.mean(times))
+    v = 1.0 / t
+    sample = (f"per step: 1 of 4 load-case Jacobi-CG solves to 1e-8 (full), 25 of the reference's 500 "
+              f"Jacobi-LOBPCG iterations (6 modes), filter/sensitivity/OC work; extrapolated to one "
+              f"iteration (last step: CG {info['t_static_s']:.2f} s, LOBPCG sample {info['t_lobpcg_sample_s']:.2f} s)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "iter/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [110, 14, 12], "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- #
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in out.strip().splitlines():
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def l2_flush(buf):
+    buf.add_(1.0)
+
+
+def time_steps(fn, n, flush_buf, torch):
+    """Sum of per-step device times (CUDA events on the current stream); the
+    L2 flush between steps is outside the timed events."""
+    total = 0.0
+    per = []
+    for _ in range(n):
+        l2_flush(flush_buf)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        dt = e0.elapsed_time(e1) / 1e3
+        per.append(dt)
+        total += dt
+    return total, per
+
+
+def measure_kernel(ctx, torch, L, R=4, reps=50):
+    """Average device time of the fine-level FP32 matvec (the multigrid
+    smoother kernel) over `reps` back-to-back launches replayed from a CUDA
+    graph, so host overhead does not enter."""
+    x = ctx.pack(torch.randn(R, ctx.N, dtype=torch.float64, device=ctx.device), dtype=torch.float32)
+    y = torch.empty_like(x)
+    lib = ctx.lib
+    s = torch.cuda.current_stream()
+    for _ in range(3):
+        lib.tof_matvec(ctx.h, L.OP_K, L.F32, L.ptr(x), L.ptr(y), R, L.c_void_p(s.cuda_stream))
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        cs = L.c_void_p(torch.cuda.current_stream().cuda_stream)
+        for _ in range(reps):
+            lib.tof_matvec(ctx.h, L.OP_K, L.F32, L.ptr(x), L.ptr(y), R, cs)
+    g.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(4):
+        g.replay()
+    e1.record()
+    e1.synchronize()
+    per_launch = e0.elapsed_time(e1) / 1e3 / (4 * reps)
+    del g
+    return per_launch
+
+
+def solver_comparison(torch, L, C):
+    """PCG / LOBPCG on the hollow-box arm in both forms, errors vs the
+    reference's FP64 results."""
+    from tof_b200.workloads import arm_hollow_analysis
+    from tof_b200.modal import effective_mass_voxel
+    golden = dict(np.load(os.path.join(ROOT, "tests", "golden", "arm.npz")))
+    out = {}
+    for form in ("mixed", "fp64"):
+        geom, fem, rho, F = arm_hollow_analysis(mode=form)
+        fem.SOLVE_RTOL = 1e-8
+        R = 4 if form == "mixed" else 1
+        fem.solve_block(rho, [F] * R, rtol=1e-8)              # warm (graph capture, multigrid setup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        us, st = fem.solve_block(rho, [F] * R, rtol=1e-8)
+        torch.cuda.synchronize()
+        t_pcg = time.perf_counter() - t0
+        c = float(F @ us[0])
+        t0 = time.perf_counter()
+        freqs, modes, lam = fem.modal_analysis(rho, n_modes=6, tip_mass_kg=C.TIP_MASS_KG, tol=1e-5)
+        torch.cuda.synchronize()
+        t_lob = time.perf_counter() - t0
+        lst = fem.last_stats
+        eff = effective_mass_voxel(fem, geom, rho, modes, C.TIP_MASS_KG, direction=2)
+        out[form] = {
+            "pcg_s": t_pcg, "pcg_rhs": R, "pcg_iters": st[0]["iters"], "pcg_relres": st[0]["relres"],
+            "compliance_rel_err": abs(c / float(golden["compliance"]) - 1.0),
+            "lobpcg_s": t_lob, "lobpcg_iters": lst["iters"], "lobpcg_max_rel_resid": lst["relres"],
+            "freq_rel_err_max": float(np.max(np.abs(freqs / golden["freqs"] - 1.0))),
+            "eff_mass_abs_err_max": float(np.max(np.abs(eff - golden["eff"]))),
+        }
+        fem.device().close()
+    return out
+
+
+def own_arm(a, rank, world, local_rank):
+    import torch
+    from tof_b200 import _lib as L
+    from tof_b200 import configs as C
+    from tof_b200.workloads import arm_simp
+
+    torch.cuda.set_device(local_rank)
+    lib = L.load()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    geom, fem, opt = arm_simp(mode="mixed")
+    for _ in range(a.warmup):
+        opt.step()
+    torch.cuda.synchronize()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
+    flush.zero_()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    n0 = lib.tof_launch_count()
+    total, per = time_steps(opt.step, a.steps, flush, torch)
+    launches = lib.tof_launch_count() - n0
+    torch.cuda.synchronize()
+    if world > 1:
+        t = torch.tensor([total], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total = float(t.item())
+        torch.distributed.barrier()
+    clocks = sampler.stop() if sampler else None
+    value = world * a.steps / total
+    hist = opt.history
+
+    # ---- end to end through the public API with host buffers
+    n_design = int(opt.design_ids.numel())
+    x_host = torch.empty(n_design, dtype=torch.float64, pin_memory=True)
+    x_host.copy_(opt.x[opt.design_ids].cpu())
+    F_host = torch.from_numpy(np.stack(opt.F_list)).pin_memory()
+    out_host = torch.empty(n_design, dtype=torch.float64, pin_memory=True)
+
+    def e2e_step():
+        xd = x_host.to("cuda", non_blocking=True)
+        opt.x[opt.design_ids] = xd
+        opt.b4 = opt.ctx.pack(F_host.to("cuda", non_blocking=True))
+        opt.step()
+        out_host.copy_(opt.x[opt.design_ids], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        x_host.copy_(out_host)
+
+    n_e2e = max(1, min(a.steps, 5))
+    e2e_total, _ = time_steps(e2e_step, n_e2e, flush, torch)
+    if world > 1:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e = {"value": world * n_e2e / e2e_total, "unit": "iter/s",
+           "h2d_bytes_per_step": int(n_design * 8 + F_host.numel() * 8),
+           "d2h_bytes_per_step": int(n_design * 8 + 8 * 4)}
+
+    # ---- dominant kernel roofline (fine-level FP32 matvec, 4 vectors)
+    ctx = opt.ctx
+    t_k = measure_kernel(ctx, torch, L, R=4)
+    Ne, NN, Rv = ctx.NE, ctx.NN, 4
+    alg_bytes = 4 * (2 * 3 * NN * Rv) + 4 * Ne            # u read + y written (3 comps), one factor per element
+    alg_flops = 1152 * Ne * Rv
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    achieved = alg_bytes / t_k / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_src,
+                "kernel": "k_matvec<float,4>: fine-level matrix-free K x (multigrid smoother / residual)",
+                "launch_us": t_k * 1e6, "algorithmic_bytes_per_launch": alg_bytes,
+                "flops_per_launch": alg_flops, "achieved_fp32_tflops": alg_flops / t_k / 1e12}
+
+    line = {"metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": total / a.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [geom.nx, geom.ny, geom.nz], "dofs": geom.n_dofs,
+                       "load_cases": len(opt.F_list), "modes": opt.n_modes_track, "pcg_rtol": 1e-8,
+                       "l2": "flushed between timed steps (256 MiB write outside the timed events)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": e2e, "roofline": roofline, "gpu_launches": int(launches),
+            "step_ms": [p * 1e3 for p in per],
+            "history": {"compliance": hist["compliance"][-a.steps:], "omega_1_Hz": hist["omega_1_Hz"][-a.steps:]}}
+    if clocks:
+        line["clocks"] = clocks
+
+    if rank == 0 and world == 1 and not a.no_extras:
+        # plain FP64 form of the same iteration (Jacobi PCG per load case, Jacobi LOBPCG)
+        _, fem64, opt64 = arm_simp(mode="fp64", batch_loads=False)
+        opt64.step()
+        torch.cuda.synchronize()
+        t64, _ = time_steps(opt64.step, 1, flush, torch)
+        line["fp64_plain"] = {"iter_s": 1.0 / t64, "ms_per_step": t64 * 1e3, "steps": 1}
+        line["speedup_mixed_vs_fp64"] = value / (1.0 / t64)
+        fem64.device().close()
+        line["solvers_hollow_arm"] = solver_comparison(torch, L, C)
+        # the reference algorithm on the host cores (bounded sample)
+        from oracle.cpu_bench import simp_iteration_sample
+        rho = C.arm_hollow_density(geom)
+        F = C.arm_static_loads(geom)
+        info = simp_iteration_sample(geom, C.PA12.E, C.PA12.nu, C.PA12.rho, rho, F + [F[0]], C.TIP_MASS_KG,
+                                     geom.motor_mount_top_nodes(), n_modes=6, lob_iters=25,
+                                     design_mask=geom.build_masks()["design"])
+        line["cpu_baseline"] = {
+            "value": 1.0 / info["t_iter_s"], "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"oracle (SciPy) reference algorithm on the arm grid: 1 of 4 load-case Jacobi-CG "
+                       f"solves to 1e-8 ({info['t_static_s']:.2f} s), 25 of 500 Jacobi-LOBPCG iterations "
+                       f"({info['t_lobpcg_sample_s']:.2f} s), element/filter/OC work; extrapolated to one "
+                       f"iteration = {info['t_iter_s']:.1f} s; SciPy sparse products are single-threaded")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        backend = "nccl" if a.impl == "own" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    try:
+        if a.impl == "reference":
+            reference_arm(a, rank, world)
+        else:
+            own_arm(a, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

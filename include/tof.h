@@ -76,6 +76,9 @@ typedef struct {
 } tof_simp_params;
 
 int tof_version(void);
+/* Number of CUDA kernels this library has launched in the process (CUDA-graph
+ * replays count their kernel nodes).  Diagnostics; no reference counterpart. */
+long long tof_launch_count(void);
 const char* tof_last_error(const tof_ctx* ctx);   /* ctx may be NULL: last create error */
 
 /* Create a design context on the current CUDA device.

@@ -69,6 +69,15 @@ bool encode_node4_map(CUtensorMap* m, const void* base, const Grid& g, int R, bo
 
 static int pow2ceil(int r) { return r <= 1 ? 1 : r <= 2 ? 2 : r <= 4 ? 4 : 8; }
 
+long long& launch_counter() {
+  static long long n = 0;
+  return n;
+}
+bool& capturing() {
+  static thread_local bool f = false;
+  return f;
+}
+
 }  // namespace tof
 
 using namespace tof;
@@ -117,6 +126,8 @@ static void free_ctx(Ctx& c) {
 extern "C" {
 
 int tof_version(void) { return 100; }
+
+long long tof_launch_count(void) { return launch_counter(); }
 
 const char* tof_last_error(const tof_ctx* ctx) {
   return ctx ? ctx->c.last_error.c_str() : g_create_error.c_str();

@@ -71,6 +71,7 @@ struct MG {
   int* info = nullptr;
   // captured PCG iterations (kGraphIters per graph), one per R = 1, 2, 4, 8
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t gnodes[4] = {0, 0, 0, 0};
   bool graph_failed = false;
 };
 constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
@@ -642,27 +643,34 @@ int mg_setup(Ctx& c, cudaStream_t s) {
     a.fx = C.fx; a.fy = C.fy; a.fz = C.fz;
     a.Ae_c = C.Ae;
     k_mg_galerkin<<<C.NE, 128, 0, s>>>(a);
+    count_launch();
     k_mg_diag<<<ceil_div(C.NN, 128), 128, 0, s>>>(C.nx, C.ny, C.nz, C.Ae, C.dinv, C.fix);
+    count_launch();
   }
   const MGLevel& L = mg->L[mg->nlev - 1];
   k_mg_coarse_setup<<<1, 256, 0, s>>>(L.nx, L.ny, L.nz, mg->nlev > 1 ? L.Ae : nullptr, c.fK64, c.Ke64, L.fix, mg->A,
                                       mg->Y, mg->Ainv, mg->info);
+  count_launch();
   // smoothing weights: power iteration on D^-1 A_l (scratch: the level's e, e2)
   for (int k = 0; k < mg->nlev - 1; ++k) {
     MGLevel& V = mg->L[k];
     float* x = V.e;
     float* y = V.e2;
     k_mg_power_init<<<ceil_div(V.NN, 256), 256, 0, s>>>(V.NN, V.fix, x);
+    count_launch();
     for (int it = 0; it < kPowerIters; ++it) {
       if (k == 0) {
         if (launch_matvec(c, 0, false, x, y, 1, nullptr, s)) return -2;
         k_mg_scale_dinv<<<ceil_div(V.NN, 256), 256, 0, s>>>(V.NN, V.dinv, y);
+        count_launch();
       } else {
         k_mgc_op<1><<<ceil_div(V.NN, 128), 128, 0, s>>>(view(V), x, nullptr, y, nullptr, 2);
+        count_launch();
       }
       std::swap(x, y);
     }
     k_mg_lambda<<<1, 1024, 0, s>>>(V.NN, y, x, mg->lam + k, mg->omega + k, kOmegaScale);
+    count_launch();
   }
   mg->dirty = false;
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
@@ -688,19 +696,22 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
     MGLevel& L = mg->L[k];
     const float* om = mg->omega + k;
     k_mg_jacobi0<<<ceil_div(L.NN * R, 256), 256, 0, s>>>(L.NN, R, L.dinv, L.r, cur[k], om);
+    count_launch();
     for (int sw = 1; sw < mg->nu; ++sw) {
       if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
-      else k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1);
+      else { k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1); count_launch(); }
       std::swap(cur[k], alt[k]);
     }
     if (k == 0) { if (launch_matvec(c, 0, false, cur[k], L.t, R, L.r, s)) return -2; }
-    else k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, L.t, nullptr, 0);
+    else { k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, L.t, nullptr, 0); count_launch(); }
     MGLevel& C = mg->L[k + 1];
     k_mg_restrict<R><<<grid1(C.NN), 128, 0, s>>>(transfer(L, C), L.t, C.fix, C.r);
+    count_launch();
   }
   {
     MGLevel& L = mg->L[nl - 1];
     k_mg_coarse_solve<<<1, 256, 0, s>>>(L.NN, R, mg->Ainv, L.r, L.e);
+    count_launch();
     cur[nl - 1] = L.e;
   }
   // upward
@@ -708,10 +719,11 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
     MGLevel& L = mg->L[k];
     MGLevel& C = mg->L[k + 1];
     k_mg_prolong<R><<<grid1(L.NN), 128, 0, s>>>(transfer(L, C), cur[k + 1], L.fix, cur[k]);
+    count_launch();
     const float* om = mg->omega + k;
     for (int sw = 0; sw < mg->nu; ++sw) {
       if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
-      else k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1);
+      else { k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1); count_launch(); }
       std::swap(cur[k], alt[k]);
     }
   }
@@ -723,6 +735,7 @@ int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
   if (c.mg->nlev == 1) {
     MGLevel& L = c.mg->L[0];
     k_mg_coarse_solve<<<1, 256, 0, s>>>(L.NN, R, c.mg->Ainv, L.r, L.e);
+    count_launch();
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
   }
   switch (R) {
@@ -987,10 +1000,13 @@ static int mgpcg_iter(Ctx& c, int pc, cudaStream_t s) {
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<c.g.ntiles, c.g.TX * c.g.TY * c.g.TZ, smem, s>>>(tmz, tmp, c.g, c.fK64, c.keb64, c.fix, mg->p[pc ^ 1], mg->q,
                                                            mg->S, mg->flags, mg->part, mg->cnt + 0);
+  count_launch();
   k_mgpcg_xr<R><<<eb, 256, 0, s>>>(c.g.NN, mg->p[pc ^ 1], mg->q, mg->x, mg->r, mg->L[0].r, mg->S, mg->flags, mg->part,
                                    mg->cnt + 1);
+  count_launch();
   if (mg_vcycle(c, R, s)) return -2;
   k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->L[0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 0);
+  count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -1008,8 +1024,10 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
   const int eb = std::min(ceil_div(c.g.NN, 256), 2 * c.num_sms);
   k_mgpcg_init<R><<<eb, 256, 0, s>>>(c.g.NN, b, mg->r, mg->L[0].r, mg->p[0], mg->S, mg->flags, mg->part, mg->cnt + 3,
                                      rtol);
+  count_launch();
   if (mg_vcycle(c, R, s)) return -2;
   k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->L[0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 1);
+  count_launch();
   int it = 0;
   int hf[9];
   const int ri = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : 3;
@@ -1024,10 +1042,12 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
     if (!mg->gexec[ri] && !mg->graph_failed) {
       cudaGraph_t graph = nullptr;
       bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      capturing() = ok;
       for (int q = 0; ok && q < kGraphIters; ++q) ok = mgpcg_iter<R>(c, q & 1, s) == 0;
+      capturing() = false;
       const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
       if (ok && ended && graph && cudaGraphInstantiate(&mg->gexec[ri], graph, 0) == cudaSuccess) {
-        // captured
+        cudaGraphGetNodes(graph, nullptr, &mg->gnodes[ri]);
       } else {
         mg->gexec[ri] = nullptr;
         mg->graph_failed = true;
@@ -1037,6 +1057,7 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
     }
     if (mg->gexec[ri]) {
       if (cudaGraphLaunch(mg->gexec[ri], s) != cudaSuccess) { c.last_error = "multigrid PCG: graph launch"; return -2; }
+      count_launch((long long)mg->gnodes[ri]);
     } else {
       for (int q = 0; q < kGraphIters; ++q)
         if (mgpcg_iter<R>(c, q & 1, s)) return -2;

@@ -12,6 +12,14 @@
 
 namespace tof {
 
+// Host-side count of kernels this library launched (graph replays add their
+// node count; launches recorded into a graph being captured are not counted).
+long long& launch_counter();
+bool& capturing();
+inline void count_launch(long long n = 1) {
+  if (!capturing()) launch_counter() += n;
+}
+
 struct MG;
 
 struct SimpParams {

@@ -29,6 +29,7 @@ __global__ void k_factors(int NE, const double* __restrict__ rho, const uint8_t*
 void launch_factors(Ctx& c, const double* rho, cudaStream_t s) {
   const int NE = c.g.NE;
   k_factors<<<ceil_div(NE, 256), 256, 0, s>>>(NE, rho, c.active, c.sp, c.fK64, c.fM64, c.fK32, c.fM32);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -75,6 +76,7 @@ __global__ void k_diag(Grid g, const double* __restrict__ fK, const double* __re
 void launch_diag(Ctx& c, cudaStream_t s) {
   k_diag<<<ceil_div(c.g.NN, 256), 256, 0, s>>>(c.g, c.fK64, c.fM64, c.Ke64, c.Me64, c.fix, c.tip64, c.dK64,
                                                  c.dM64, c.dinvK64, c.dinvK32);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -182,6 +184,7 @@ static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b
   auto kern = k_matvec<T, R>;
   if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   kern<<<c.g.ntiles, c.g.TX * c.g.TY * c.g.TZ, smem, s>>>(tm, a);
+  count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -263,6 +266,7 @@ void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool 
   const int blocks = int((n + 255) / 256);
   if (f64) k_pack<double><<<blocks, 256, 0, s>>>(c.g.NN, nvec, src, ld, c.fix, (double*)dst);
   else k_pack<float><<<blocks, 256, 0, s>>>(c.g.NN, nvec, src, ld, c.fix, (float*)dst);
+  count_launch();
 }
 
 void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s) {
@@ -270,6 +274,7 @@ void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long lo
   const int blocks = int((n + 255) / 256);
   if (f64) k_unpack<double><<<blocks, 256, 0, s>>>(c.g.NN, nvec, (const double*)src, dst, ld);
   else k_unpack<float><<<blocks, 256, 0, s>>>(c.g.NN, nvec, (const float*)src, dst, ld);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -353,7 +358,9 @@ void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb,
   else
     k_gram_partial<float, 32><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, na, (const float*)B, nb,
                                                               vs, c.gram_part);
+  count_launch();
   k_gram_reduce<<<ceil_div(na * nb, 128), 128, 0, s>>>(blocks, na * nb, c.gram_part, G);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -403,6 +410,7 @@ void launch_quadform(const Ctx& c, int op, bool f64, const void* v, int nvec, do
   const int blocks = ceil_div(c.g.NE, 256);
   if (f64) k_quadform<double><<<blocks, 256, 0, s>>>(c.g, (const double*)v, nvec, vs, A, c.active, out);
   else k_quadform<float><<<blocks, 256, 0, s>>>(c.g, (const float*)v, nvec, vs, A, c.active, out);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -420,6 +428,7 @@ void launch_convert(const void* src, bool src64, void* dst, bool dst64, long lon
   else if (!src64 && dst64) k_convert<float, double><<<blocks, 256, 0, s>>>((const float*)src, (double*)dst, n);
   else if (src64) k_convert<double, double><<<blocks, 256, 0, s>>>((const double*)src, (double*)dst, n);
   else k_convert<float, float><<<blocks, 256, 0, s>>>((const float*)src, (float*)dst, n);
+  count_launch();
 }
 
 __global__ void k_axpy64(long long n, const double* __restrict__ x, double* y, double a) {
@@ -428,6 +437,7 @@ __global__ void k_axpy64(long long n, const double* __restrict__ x, double* y, d
 }
 void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s) {
   k_axpy64<<<int((n + 255) / 256), 256, 0, s>>>(n, x, y, a);
+  count_launch();
 }
 
 __global__ void k_add_f32_to_f64(long long n, const float* __restrict__ d, double* x) {
@@ -436,6 +446,7 @@ __global__ void k_add_f32_to_f64(long long n, const float* __restrict__ d, doubl
 }
 void launch_add_f32_to_f64(long long n, const float* d, double* x, cudaStream_t s) {
   k_add_f32_to_f64<<<int((n + 255) / 256), 256, 0, s>>>(n, d, x);
+  count_launch();
 }
 
 }  // namespace tof

@@ -288,6 +288,7 @@ static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s) {
   double* th = c.gram + 3 * 576;
   int* info = c.status + 8;
   k_small_eig<<<1, 32, 0, s>>>(n, m, GK, GM, drop, C, th, info);
+  count_launch();
   return 0;
 }
 
@@ -330,6 +331,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   lob_small_eig(c, nb, nb, drop, s);
   k_lob_update<T><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, nb, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
                                                      (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1]);
+  count_launch();
   cur ^= 1;
   int it = 0;
   double hr[16];
@@ -345,7 +347,9 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
     k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, W, c.gram_part);
+    count_launch();
     k_lob_resid_reduce<<<1, 32, 0, s>>>(rblocks, c.gram_part, rn);
+    count_launch();
     cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
@@ -391,6 +395,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     k_lob_update<T><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, ncols, vs, (T*)B.S[cur], (T*)B.KS[cur],
                                                        (T*)B.MS[cur], C, (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1],
                                                        (T*)B.MS[cur ^ 1]);
+    count_launch();
     cur ^= 1;
     (void)X;
   }
@@ -415,6 +420,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     k_lob_update<double><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, nb, vs, X6, KX6, MX6, C, scratch,
                                                             scratch + 3LL * c.max_modes * vs,
                                                             scratch + 6LL * c.max_modes * vs);
+    count_launch();
     cudaMemcpyAsync(out, scratch, sizeof(double) * nmodes * vs, cudaMemcpyDeviceToDevice, s);
   }
   cudaMemcpyAsync(hth, th, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);

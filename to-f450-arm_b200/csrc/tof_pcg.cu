@@ -594,6 +594,7 @@ static int pipe_launch(Ctx& c, const double* b, float* d, double rtol, int maxit
   void* args[] = {(void*)&a};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(c.g.TX * c.g.TY * c.g.TZ), args,
                                               smem, s);
+  count_launch();
   if (e != cudaSuccess) { c.last_error = cudaGetErrorString(e); return -2; }
   return 0;
 }
@@ -632,6 +633,7 @@ static int plain_launch(Ctx& c, const double* b, T* x, double rtol, int maxiter,
   void* args[] = {(void*)&a};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(c.g.TX * c.g.TY * c.g.TZ), args,
                                               smem, s);
+  count_launch();
   if (e != cudaSuccess) { c.last_error = cudaGetErrorString(e); return -2; }
   return 0;
 }

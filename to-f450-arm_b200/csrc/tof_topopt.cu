@@ -72,6 +72,7 @@ void launch_filter_den(int nx, int ny, int nz, const void* taps, int ntaps, cons
                        cudaStream_t s) {
   const int NE = nx * ny * nz;
   k_filter_den<<<ceil_div(NE, 256), 256, 0, s>>>(nx, ny, nz, (const FilterTap*)taps, ntaps, mask, den);
+  count_launch();
 }
 
 void launch_filter(int nx, int ny, int nz, const void* taps, int ntaps, const uint8_t* mask, const double* den,
@@ -79,6 +80,7 @@ void launch_filter(int nx, int ny, int nz, const void* taps, int ntaps, const ui
   const int NE = nx * ny * nz;
   k_filter<<<ceil_div(NE, 256), 256, ntaps * sizeof(FilterTap), s>>>(nx, ny, nz, (const FilterTap*)taps, ntaps,
                                                                       mask, den, fill, in, out, mode);
+  count_launch();
 }
 
 size_t filter_tap_bytes() { return sizeof(FilterTap); }
@@ -121,6 +123,7 @@ __global__ void __launch_bounds__(1024) k_oc(int n, const double* __restrict__ x
 void launch_oc(int n, const double* x, const double* dc, double V_e, double target, double move, double* x_new,
                int* n_bisect, cudaStream_t s) {
   k_oc<<<1, 1024, 0, s>>>(n, x, dc, V_e, target, move, x_new, n_bisect);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -170,7 +173,9 @@ void launch_compliance_sens(int NE, int nlc, const double* w, const double* rho,
                             cudaStream_t s) {
   const int blocks = ceil_div(NE, 256);
   k_compliance_sens<<<blocks, 256, 0, s>>>(NE, nlc, w, rho, ce, active, sp, dc, part);
+  count_launch();
   k_sum_partials<<<1, 256, 0, s>>>(blocks, part, c_out);
+  count_launch();
 }
 
 __global__ void k_mass_quad(int NE, const double* __restrict__ rho, const double* __restrict__ qM,
@@ -210,8 +215,11 @@ void launch_eig_sens(int NE, const double* rho, const double* qK, const double* 
                      cudaStream_t s) {
   const int blocks = ceil_div(NE, 256);
   k_mass_quad<<<blocks, 256, 0, s>>>(NE, rho, qM, active, sp, part);
+  count_launch();
   k_sum_partials<<<1, 256, 0, s>>>(blocks, part, scal);
+  count_launch();
   k_eig_sens<<<blocks, 256, 0, s>>>(NE, rho, qK, qM, active, sp, lam, scal, vMv_tip, out);
+  count_launch();
 }
 
 }  // namespace tof

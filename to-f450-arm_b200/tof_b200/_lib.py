@@ -44,6 +44,7 @@ P = c_void_p
 # name -> (restype, argtypes); the complete list of exported entry points
 SIGNATURES = {
     "tof_version": (c_int, []),
+    "tof_launch_count": (c_longlong, []),
     "tof_last_error": (ctypes.c_char_p, [P]),
     "tof_ctx_create": (c_int, [c_int, c_int, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_double),
                                POINTER(c_uint8), POINTER(c_uint8), POINTER(c_double), POINTER(SimpParams),

@@ -1,0 +1,48 @@
+"""Ready-made workloads on the synthetic arm / cantilever domains.
+
+`arm_simp(...)` builds the design-iteration workload: the 2 mm arm grid
+(110 x 14 x 12 voxels), four load cases (15 N -z thrust on the motor-mount
+face; 0.3 N m torque about the arm axis plus 10 N lateral on the tip face;
+both together; a 3 g -z inertial load from the consistent mass at the
+starting design), 6 tracked modes with a 500 Hz augmented-Lagrangian target,
+60 g tip mass, filter radius 1.5 voxels, vf 0.08, design start
+0.08 + U(-0.02, 0.02) (seed 0), static solves to a 1e-8 relative residual.
+The inertial load is evaluated once at the starting design and then held
+fixed, as the reference's optimiser supports design-independent loads only.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import configs as C
+from .fem import FEM3D
+from .topopt import SIMPOptimizer
+
+
+def arm_simp(mode="mixed", nx=110, ny=14, nz=12, h=2e-3, vf=0.08, n_modes=6, min_freq_Hz=500.0,
+             solve_rtol=1e-8, modal_tol=1e-5, batch_loads=True, seed=0, tile=None):
+    geom = C.arm_geometry(nx=nx, ny=ny, nz=nz, h=h)
+    fem = FEM3D(geom, C.PA12, mode=mode, tile=tile)
+    F3 = C.arm_static_loads(geom)
+    x0 = C.arm_design_start(geom, vf=vf, seed=seed).astype(np.float64)
+    opt = SIMPOptimizer(geom, fem, load_cases=[], vol_frac=vf, r_min_mm=3.0 * h / 2e-3, move=0.2,
+                        max_iter=50, tol_change=0.0, min_freq_Hz=min_freq_Hz, tip_mass_kg=C.TIP_MASS_KG,
+                        n_modes_track=n_modes, mu_freq_init=0.2, mu_freq_max=50.0, mu_freq_ramp_every=5,
+                        mu_freq_ramp_factor=1.5, batch_loads=batch_loads, solve_rtol=solve_rtol,
+                        modal_tol=modal_tol, x0_design=x0, F_list=F3 + [np.zeros(geom.n_dofs)])
+    rho0 = opt.physical_density()
+    rho_active = rho0[torch.as_tensor(fem.active_ids, device=rho0.device)].cpu().numpy()
+    ez = np.zeros(geom.n_dofs)
+    ez[2::3] = 1.0
+    Mr = fem.assemble_M(rho_active, C.TIP_MASS_KG, geom.motor_mount_top_nodes()) @ ez
+    opt.set_loads(F3 + [C.body_load_from_Mr(Mr, 3.0)])
+    return geom, fem, opt
+
+
+def arm_hollow_analysis(mode="mixed", tile=None):
+    """The hollow-box arm (1-voxel walls at 1.0, core 1e-3), thrust load,
+    60 g tip mass: (geom, fem, rho_active, F)."""
+    geom = C.arm_geometry()
+    fem = FEM3D(geom, C.PA12, mode=mode, tile=tile)
+    return geom, fem, C.arm_hollow_density(geom), C.arm_static_loads(geom)[0]
