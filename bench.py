@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="own", choices=["own", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip FP64/solver/CPU comparisons")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer and kernel-roofline runs "
+                    "(profiling runs)")
     return ap.parse_args()
 
 
@@ -256,6 +258,12 @@ def own_arm(a, rank, world, local_rank):
     value = world * a.steps / total
     hist = opt.history
 
+    if a.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
+                              "steps": a.steps, "warmup": a.warmup, "ms_per_step": total / a.steps * 1e3,
+                              "gpu_launches": int(launches), "profiling_run": True}), flush=True)
+        return
     # ---- end to end through the public API with host buffers
     n_design = int(opt.design_ids.numel())
     x_host = torch.empty(n_design, dtype=torch.float64, pin_memory=True)

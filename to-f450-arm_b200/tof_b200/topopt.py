@@ -61,6 +61,7 @@ class SIMPOptimizer:
       solve_rtol   - static solve tolerance (default fem.SOLVE_RTOL);
       modal_tol    - LOBPCG relative residual tolerance (default 1e-5);
       x0_design    - start values on the design cells (reference order);
+      modal_maxiter - LOBPCG iteration cap (default 20000 Jacobi / 1000 multigrid);
       F_list       - explicit full-length load vectors instead of load_cases.
     """
 
@@ -69,7 +70,7 @@ class SIMPOptimizer:
                  min_freq_Hz: float = None, tip_mass_kg: float = 0.060, n_modes_track: int = 4,
                  mu_freq_init: float = 0.10, mu_freq_max: float = 50.0, mu_freq_ramp_every: int = 5,
                  mu_freq_ramp_factor: float = 1.5, batch_loads: bool = True, solve_rtol: float = None,
-                 modal_tol: float = 1e-5, x0_design=None, F_list=None):
+                 modal_tol: float = 1e-5, x0_design=None, F_list=None, modal_maxiter: int = None):
         self.geom, self.fem = geom, fem
         self.load_cases = load_cases
         self.vol_frac = vol_frac
@@ -83,6 +84,7 @@ class SIMPOptimizer:
         self.batch_loads = batch_loads
         self.solve_rtol = fem.SOLVE_RTOL if solve_rtol is None else solve_rtol
         self.modal_tol = modal_tol
+        self.modal_maxiter = modal_maxiter
         n_lc = len(F_list) if F_list is not None else len(load_cases)
         w = np.full(n_lc, 1.0 / n_lc) if weights is None else np.asarray(weights, dtype=float)
         self.weights = w / w.sum()                                           # src/topopt.py:121-124
@@ -132,7 +134,11 @@ class SIMPOptimizer:
         self.modal_active = self.min_freq_Hz is not None
         self.tip_nodes = fem._tip_nodes(None) if self.modal_active else np.array([], dtype=np.int64)
         tip = fem.tip_lump(self.tip_mass_kg, self.tip_nodes) if self.modal_active else None
+        self._tip3 = tip
+        self._tip_key = None if tip is None else tip.tobytes()
         self.tip4 = ctx.pack(torch.from_numpy(np.zeros(geom.n_dofs) if tip is None else tip))[0]
+        self.profile = False          # True: synchronised per-phase timings in self.phase_times
+        self.phase_times = {}
         self.lam_t = (2.0 * np.pi * self.min_freq_Hz) ** 2 if self.modal_active else None
         self.reset()
 
@@ -160,10 +166,21 @@ class SIMPOptimizer:
         self.it = 0
         self.mu_freq_cur = self.mu_freq
         self.history = {"compliance": [], "mass": [], "change": [], "vol_frac": [], "omega_1_Hz": [],
-                        "mu_freq": [], "freq_violation": []}
+                        "mu_freq": [], "freq_violation": [], "modal_converged": [], "modal_iters": [],
+                        "pcg_iters": []}
         self.stats = []
 
     # ------------------------------------------------------------------ #
+    def _mark(self, name):
+        """Phase timer (only when self.profile is set; synchronises)."""
+        if not self.profile:
+            return
+        torch.cuda.synchronize()
+        now = time.perf_counter()
+        if name is not None:
+            self.phase_times[name] = self.phase_times.get(name, 0.0) + now - self._t_mark
+        self._t_mark = now
+
     def physical_density(self, x=None) -> torch.Tensor:
         """Filtered design, keep-solid = 1, inactive = 0 (src/topopt.py:270-281)."""
         return self.filter.apply(self.x if x is None else x, L.FILTER_PHYSICAL)
@@ -182,11 +199,14 @@ class SIMPOptimizer:
         else:
             X4 = self.X4
         mid = fem._mode_id()
-        modes, lam, st = ctx.lobpcg(X4, n, tol=self.modal_tol, maxiter=5000 if mid == L.MODE_FP64 else 1000,
-                                    mode=mid, precond=L.PRECOND_MG if mid == L.MODE_MIXED else L.PRECOND_JACOBI)
+        maxit = self.modal_maxiter or (20000 if mid == L.MODE_FP64 else 1000)
+        modes, lam, st = ctx.lobpcg(X4, n, tol=self.modal_tol, maxiter=maxit, mode=mid,
+                                    precond=L.PRECOND_MG if mid == L.MODE_MIXED else L.PRECOND_JACOBI)
         # warm start: converged modes plus the previous guard vectors
         self.X4 = torch.cat([modes, X4[n:]]) if nb > n else modes.clone()
         self.stats.append(("lobpcg", st))
+        self.history["modal_converged"].append(st["status"] == L.TOF_OK)
+        self.history["modal_iters"].append(st["iters"])
         return modes, np.maximum(lam, 0.0)
 
     def step(self):
@@ -196,15 +216,14 @@ class SIMPOptimizer:
         t0 = time.time()
         fem, ctx = self.fem, self.ctx
         p, emin = fem.SIMP_PENALTY, fem.E_MIN_FRAC
+        self._mark(None)
         rho = self.physical_density()
         ctx.set_density(rho)
         fem._rho_dev = None                                  # the FEM3D cache no longer matches
-        if self.modal_active:
-            t = fem.tip_lump(self.tip_mass_kg, self.tip_nodes)
-            key = None if t is None else t.tobytes()
-            if fem._tip_key != key or fem._tip_key is None:
-                ctx.set_tip_lump(t)
-                fem._tip_key = key
+        if self.modal_active and (fem._tip_key is None or fem._tip_key != self._tip_key):
+            ctx.set_tip_lump(self._tip3)
+            fem._tip_key = self._tip_key
+        self._mark("filter+density")
         # --- all load cases (src/topopt.py:287-306)
         mid = fem._mode_id()
         R = self.b4.shape[0]
@@ -220,13 +239,17 @@ class SIMPOptimizer:
             u4 = torch.cat(parts)
         self.u4 = u4
         self.stats.append(("pcg", st))
+        self.history["pcg_iters"].append(max(s["iters"] for s in st))
+        self._mark("static solves")
         ce = ctx.quadform(L.OP_K, u4)
         c_dev, dc = ctx.compliance_sens(ce, self.w_dev)
         sens = self.filter.apply(dc, L.FILTER_FORWARD)       # src/topopt.py:311
         c_total = float(c_dev.item())
+        self._mark("compliance sens+filter")
         # --- modal constraint (src/topopt.py:313-375)
         if self.modal_active:
             modes, lam = self._modal(rho)
+            self._mark("modal solve")
             if self.v_prev is None:
                 k = 0
             else:                                            # MAC, src/topopt.py:179-188
@@ -257,6 +280,7 @@ class SIMPOptimizer:
         else:
             for k in ("omega_1_Hz", "mu_freq", "freq_violation"):
                 self.history[k].append(np.nan)
+        self._mark("eigen sens+penalty")
         # --- OC on design cells (src/topopt.py:377-390)
         x_d = self.x[self.design_ids]
         x_new_d = oc_update(x_d, sens[self.design_ids], self.V_e, self.target_volume, self.move)
@@ -270,6 +294,7 @@ class SIMPOptimizer:
         self.history["mass"].append(mass)
         self.history["change"].append(change)
         self.history["vol_frac"].append(mass / self.design_volume)
+        self._mark("OC+change")
         self.last_step_s = time.time() - t0
         return change
 
