@@ -162,6 +162,23 @@ int tof_elem_quadform(tof_ctx* ctx, int op, int dtype, const void* v, int nvec, 
 /* G = A^T B (na x nb, row-major, device FP64) of node4 blocks, na, nb <= 24. */
 int tof_gram(tof_ctx* ctx, int dtype, const void* A, int na, const void* B, int nb, double* G, void* stream);
 
+/* The same G = A^T B without a context and without allocating any device
+ * memory; no counterpart in the reference.  For callers that cannot allocate
+ * device memory when they need it: a host application whose memory pool owns
+ * the whole GPU, code issuing work while a stream is being captured into a
+ * CUDA graph (where cudaMalloc is not allowed), or a loop that must not take
+ * cudaMalloc's implicit device synchronisation.  A, B: node4 blocks of
+ * n_nodes nodes, dtype TOF_F32 or TOF_F64; G: device FP64 na x nb.
+ * Limits: na, nb <= 24 and n_nodes < 2^31, else TOF_ERR_ARG with a message in
+ * tof_last_error(NULL).  Temporaries live in one fixed device array of about
+ * 1.1 MiB that every GPU loading the library keeps until the process exits;
+ * the first call on a device looks up that array's device address (issue it
+ * before any stream capture).  All calls on a GPU share the array and it
+ * keeps the previous call's contents: calls whose executions overlap on the
+ * same GPU race, so order them (one stream, or events). */
+int tof_gram_noalloc(long long n_nodes, int dtype, const void* A, int na, const void* B, int nb, double* G,
+                     void* stream);
+
 /* Compliance and its sensitivity for nlc load cases from ce [nlc][NE]
  * (src/topopt.py:291-306): c = sum_l w_l sum_e f_e ce_le (device scalar
  * c_out), dc_e = sum_l w_l (-p (1-emin) rho_e^(p-1) ce_le) (device [NE]). */

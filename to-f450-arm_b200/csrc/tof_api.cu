@@ -96,6 +96,8 @@ struct tof_filter {
 
 static thread_local std::string g_create_error;
 
+void tof::set_global_error(const std::string& msg) { g_create_error = msg; }
+
 #define CUDA_TRY(expr)                                                    \
   do {                                                                    \
     cudaError_t _e = (expr);                                              \

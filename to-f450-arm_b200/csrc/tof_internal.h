@@ -19,6 +19,8 @@ bool& capturing();
 inline void count_launch(long long n = 1) {
   if (!capturing()) launch_counter() += n;
 }
+// Error message of calls without a context (returned by tof_last_error(NULL)).
+void set_global_error(const std::string& msg);
 
 struct MG;
 

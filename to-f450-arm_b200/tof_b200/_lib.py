@@ -62,6 +62,7 @@ SIGNATURES = {
                            POINTER(SolveStats), POINTER(c_double), P]),
     "tof_elem_quadform": (c_int, [P, c_int, c_int, P, c_int, P, P]),
     "tof_gram": (c_int, [P, c_int, P, c_int, P, c_int, P, P]),
+    "tof_gram_noalloc": (c_int, [c_longlong, c_int, P, c_int, P, c_int, P, P]),
     "tof_compliance_sens": (c_int, [P, c_int, P, P, P, P, P]),
     "tof_eig_sens": (c_int, [P, P, P, c_double, c_double, P, P]),
     "tof_effective_mass": (c_int, [P, P, c_int, c_int, POINTER(c_double), P]),
