@@ -120,7 +120,7 @@ static void free_ctx(Ctx& c) {
   mg_destroy(c);
   void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
                   c.fK64, c.fM64, c.fK32, c.fM32, c.rho, c.dK64, c.dM64, c.dinvK64, c.dinvK32, c.partials,
-                  c.bar, c.status, c.scal, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part};
+                  c.bar, c.status, c.scal, c.counters, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -232,6 +232,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.dK64, V)); A(dalloc(c, &c.dM64, V)); A(dalloc(c, &c.dinvK64, V)); A(dalloc(c, &c.dinvK32, V));
   A(dalloc(c, &c.partials, (size_t)c.partial_slots * 64));
   A(dalloc(c, &c.bar, 1)); A(dalloc(c, &c.status, 32)); A(dalloc(c, &c.scal, 256));
+  A(dalloc(c, &c.counters, 16));
   A(dalloc(c, &c.pw32, 10 * R * V));
   A(dalloc(c, &c.pw64, 8 * R * V));
   A(dalloc(c, &c.lw32, 18 * MM * V));

@@ -220,4 +220,32 @@ template <typename T> struct Vec4;
 template <> struct Vec4<float> { using type = float4; };
 template <> struct Vec4<double> { using type = double4; };
 
+// Last-block-finishes reduction: every block adds its K partial sums; the last
+// block to arrive sums all partials in block order (deterministic) into
+// `total` and returns true.
+template <int K>
+__device__ bool last_block(double (&v)[K], double* part, unsigned* counter, double* scratch, double (&total)[K]) {
+  __shared__ int s_last;
+  block_sum<K>(v, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[(size_t)blockIdx.x * K + k] = v[k];
+    __threadfence();
+    const unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; ++k) total[k] = 0.0;
+  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) total[k] += __ldcg(part + (size_t)b * K + k);
+  }
+  block_sum<K>(total, scratch);
+  if (threadIdx.x == 0) *counter = 0u;
+  return true;
+}
+
 }  // namespace tof

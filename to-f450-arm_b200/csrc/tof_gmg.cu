@@ -44,6 +44,7 @@ struct MGLevel {
   int nx, ny, nz, NX, NY, NZ, NN, NE;
   int fx, fy, fz;          // coarsening factor from the finer level (1 or 2)
   float* Ae = nullptr;     // [NE][576] Galerkin element matrices (levels >= 1)
+  float* St = nullptr;     // [243][NN] assembled node stencils (levels 1 .. nlev-2)
   float* dinv = nullptr;   // node4
   uint8_t* fix = nullptr;  // node bits
   float *r = nullptr, *e = nullptr, *e2 = nullptr, *t = nullptr;   // node4 x maxR
@@ -81,34 +82,6 @@ constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void node_ijk(int n, int NX, int NY, int& i, int& j, int& k) {
   i = n % NX; j = (n / NX) % NY; k = n / (NX * NY);
-}
-
-// Last-block-finishes reduction: every block adds its K partial sums; the last
-// block to arrive sums all partials in block order (deterministic) into
-// `total` and returns true.
-template <int K>
-__device__ bool last_block(double (&v)[K], double* part, unsigned* counter, double* scratch, double (&total)[K]) {
-  __shared__ int s_last;
-  block_sum<K>(v, scratch);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) part[(size_t)blockIdx.x * K + k] = v[k];
-    __threadfence();
-    const unsigned t = atomicAdd(counter, 1u);
-    s_last = (t == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!s_last) return false;
-  __threadfence();
-#pragma unroll
-  for (int k = 0; k < K; ++k) total[k] = 0.0;
-  for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) total[k] += __ldcg(part + (size_t)b * K + k);
-  }
-  block_sum<K>(total, scratch);
-  if (threadIdx.x == 0) *counter = 0u;
-  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -222,6 +195,41 @@ __global__ void k_mg_diag(int nx, int ny, int nz, const float* __restrict__ Ae, 
   fix[n] = f;
 }
 
+// Assembled node stencil of a coarse level: for node n and neighbour
+// nb = (dz+1)*9 + (dy+1)*3 + (dx+1), the 3x3 block coupling n to
+// n + (dx, dy, dz) is the sum over the (up to 4) elements holding both nodes
+// of Ae[E][3 ln + q][3 lm + p].  Stored structure-of-arrays,
+// St[(nb * 9 + q * 3 + p) * NN + n], so that a warp of consecutive nodes reads
+// each entry coalesced.  One thread per (node, neighbour).
+__global__ void k_mg_stencil(int nx, int ny, int nz, const float* __restrict__ Ae, float* St) {
+  const int NX = nx + 1, NY = ny + 1, NN = NX * NY * (nz + 1);
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 27LL * NN) return;
+  const int n = int(t % NN), nb = int(t / NN);
+  const int dx = nb % 3 - 1, dy = (nb / 3) % 3 - 1, dz = nb / 9 - 1;
+  int i, j, k;
+  node_ijk(n, NX, NY, i, j, k);
+  double s[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) s[e] = 0.0;
+  for (int c = -1; c <= 0; ++c)
+    for (int b = -1; b <= 0; ++b)
+      for (int a = -1; a <= 0; ++a) {
+        const int ex = i + a, ey = j + b, ez = k + c;
+        if (ex < 0 || ey < 0 || ez < 0 || ex >= nx || ey >= ny || ez >= nz) continue;
+        const int mx = dx - a, my = dy - b, mz = dz - c;   // neighbour's offset inside the element
+        if (mx < 0 || mx > 1 || my < 0 || my > 1 || mz < 0 || mz > 1) continue;
+        const int E = (ez * ny + ey) * nx + ex, ln = local_node(-a, -b, -c), lm = local_node(mx, my, mz);
+        const float* Kr = Ae + (size_t)E * 576 + (3 * ln) * 24 + 3 * lm;
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+          for (int p = 0; p < 3; ++p) s[q * 3 + p] += double(Kr[q * 24 + p]);
+      }
+#pragma unroll
+  for (int e = 0; e < 9; ++e) St[(size_t)(nb * 9 + e) * NN + n] = float(s[e]);
+}
+
 // Coarsest level: dense assembly (row per thread), Cholesky, inverse.
 // Level 0 (Ae == null) assembles from factors and Ke with the fixed mask.
 __global__ void __launch_bounds__(256) k_mg_coarse_setup(int nx, int ny, int nz, const float* __restrict__ Ae,
@@ -305,80 +313,60 @@ __global__ void __launch_bounds__(256) k_mg_coarse_setup(int nx, int ny, int nz,
 // ---------------------------------------------------------------------------
 struct LevelView {
   int nx, ny, nz, NX, NY, NZ, NN;
-  const float* Ae;
+  const float* St;
   const float* dinv;
   const uint8_t* fix;
 };
 
-template <int R>
-__device__ __forceinline__ void elem_apply(const LevelView& L, int n, const float* __restrict__ x, long long vs,
-                                           float (&acc)[R][3]) {
+// Coarse-level operator from the assembled stencil, one thread per
+// (node, output component q, right-hand side r): a CTA is 32 consecutive
+// nodes x (3 R) warps, so each warp reads the stencil rows of its q
+// coalesced and the R warps sharing them hit L1.
+// mode 0: y = b - A x;  mode 1: y = x + omega D^-1 (b - A x);  mode 2: y = D^-1 A x
+// (fixed DOFs of modes 0 and 1 are set to 0; the padding component to 0).
+__global__ void __launch_bounds__(768) k_mgs_op(LevelView L, int R, const float* __restrict__ x,
+                                                const float* __restrict__ b, float* y,
+                                                const float* __restrict__ omega_p, int mode) {
+  const int n = blockIdx.x * 32 + threadIdx.x;
+  const int q = threadIdx.y % 3, r = threadIdx.y / 3;
+  if (n >= L.NN || r >= R) return;
+  const long long vs = (long long)L.NN * 4;
   int i, j, k;
   node_ijk(n, L.NX, L.NY, i, j, k);
+  const float* xr = x + r * vs;
+  const float* S = L.St + (size_t)q * 3 * L.NN + n;
+  float acc = 0.f;
 #pragma unroll
-  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
-  for (int c = -1; c <= 0; ++c)
-    for (int b = -1; b <= 0; ++b)
-      for (int a = -1; a <= 0; ++a) {
-        const int ex = i + a, ey = j + b, ez = k + c;
-        if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
-        const int E = (ez * L.ny + ey) * L.nx + ex, ln = local_node(-a, -b, -c);
-        const float* Kr = L.Ae + (size_t)E * 576 + (3 * ln) * 24;
-#pragma unroll
-        for (int lm = 0; lm < 8; ++lm) {
-          const int mx = (lm == 1 || lm == 2 || lm == 5 || lm == 6), my = (lm == 2 || lm == 3 || lm == 6 || lm == 7),
-                    mz = lm >= 4;
-          const int M = ((ez + mz) * L.NY + (ey + my)) * L.NX + (ex + mx);
-          float k0[3], k1[3], k2[3];
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            k0[q] = __ldg(Kr + 3 * lm + q);
-            k1[q] = __ldg(Kr + 24 + 3 * lm + q);
-            k2[q] = __ldg(Kr + 48 + 3 * lm + q);
-          }
-#pragma unroll
-          for (int r = 0; r < R; ++r) {
-            const float4 xv = __ldg(reinterpret_cast<const float4*>(x + r * vs) + M);
-            acc[r][0] += k0[0] * xv.x + k0[1] * xv.y + k0[2] * xv.z;
-            acc[r][1] += k1[0] * xv.x + k1[1] * xv.y + k1[2] * xv.z;
-            acc[r][2] += k2[0] * xv.x + k2[1] * xv.y + k2[2] * xv.z;
-          }
-        }
-      }
+  for (int nb = 0; nb < 27; ++nb) {
+    const int dx = nb % 3 - 1, dy = (nb / 3) % 3 - 1, dz = nb / 9 - 1;
+    const bool in = (unsigned)(i + dx) < (unsigned)L.NX && (unsigned)(j + dy) < (unsigned)L.NY &&
+                    (unsigned)(k + dz) < (unsigned)L.NZ;
+    if (!in) continue;
+    const int m = n + (dz * L.NY + dy) * L.NX + dx;
+    const float4 xv = __ldg(reinterpret_cast<const float4*>(xr) + m);
+    const float* Sq = S + (size_t)nb * 9 * L.NN;
+    acc = fmaf(__ldg(Sq), xv.x, acc);
+    acc = fmaf(__ldg(Sq + L.NN), xv.y, acc);
+    acc = fmaf(__ldg(Sq + 2 * (size_t)L.NN), xv.z, acc);
+  }
+  const size_t o = r * vs + 4 * (size_t)n;
+  const float di = L.dinv[4 * (size_t)n + q];
+  float out;
+  if (mode == 2) {
+    out = di * acc;
+  } else {
+    out = b[o + q] - acc;
+    if (mode == 1) out = fmaf(__ldg(omega_p) * di, out, x[o + q]);
+    if ((L.fix[n] >> q) & 1) out = 0.f;
+  }
+  y[o + q] = out;
+  if (q == 0) y[o + 3] = 0.f;
 }
 
-// mode 0: y = b - A x;  mode 1: y = x + omega D^-1 (b - A x);  mode 2: y = D^-1 A x
-template <int R>
-__global__ void __launch_bounds__(128) k_mgc_op(LevelView L, const float* __restrict__ x, const float* __restrict__ b,
-                                                float* y, const float* __restrict__ omega_p, int mode) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= L.NN) return;
-  const long long vs = (long long)L.NN * 4;
-  float acc[R][3];
-  elem_apply<R>(L, n, x, vs, acc);
-  const uint8_t fx = L.fix[n];
-  const float4 di = reinterpret_cast<const float4*>(L.dinv)[n];
-  const float omega = mode == 1 ? __ldg(omega_p) : 0.f;
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    if (mode == 2) {
-      reinterpret_cast<float4*>(y + r * vs)[n] =
-          make_float4(di.x * acc[r][0], di.y * acc[r][1], di.z * acc[r][2], 0.f);
-      continue;
-    }
-    const float4 bb = reinterpret_cast<const float4*>(b + r * vs)[n];
-    float4 o = make_float4(bb.x - acc[r][0], bb.y - acc[r][1], bb.z - acc[r][2], 0.f);
-    if (mode == 1) {
-      const float4 xc = reinterpret_cast<const float4*>(x + r * vs)[n];
-      o.x = fmaf(omega * di.x, o.x, xc.x);
-      o.y = fmaf(omega * di.y, o.y, xc.y);
-      o.z = fmaf(omega * di.z, o.z, xc.z);
-    }
-    o.x = (fx & 1) ? 0.f : o.x;
-    o.y = (fx & 2) ? 0.f : o.y;
-    o.z = (fx & 4) ? 0.f : o.z;
-    reinterpret_cast<float4*>(y + r * vs)[n] = o;
-  }
+static void launch_mgs_op(const LevelView& L, int R, const float* x, const float* b, float* y, const float* om,
+                          int mode, cudaStream_t s) {
+  k_mgs_op<<<ceil_div(L.NN, 32), dim3(32, 3 * R), 0, s>>>(L, R, x, b, y, om, mode);
+  count_launch();
 }
 
 // e = omega D^-1 r  (first pre-smoothing sweep from e = 0), any level
@@ -440,18 +428,19 @@ struct Transfer {
   int fx, fy, fz;
 };
 
-// r_c = P^T t_f (masked by the coarse fixed bits)
-template <int R>
-__global__ void k_mg_restrict(Transfer T, const float* __restrict__ tf, const uint8_t* __restrict__ fixc, float* rc) {
-  const int N = blockIdx.x * blockDim.x + threadIdx.x;
+// r_c = P^T t_f (masked by the coarse fixed bits); one thread per (coarse
+// node, right-hand side)
+__global__ void k_mg_restrict(Transfer T, int R, const float* __restrict__ tf, const uint8_t* __restrict__ fixc,
+                              float* rc) {
   const int NNc = T.NXc * T.NYc * T.NZc;
-  if (N >= NNc) return;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)NNc * R) return;
+  const int N = int(t % NNc), r = int(t / NNc);
   int I, J, K;
   node_ijk(N, T.NXc, T.NYc, I, J, K);
   const long long vsf = (long long)T.NXf * T.NYf * T.NZf * 4, vsc = (long long)NNc * 4;
-  float acc[R][3];
-#pragma unroll
-  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
+  const float4* src = reinterpret_cast<const float4*>(tf + r * vsf);
+  float acc[3] = {0.f, 0.f, 0.f};
   const int dz0 = T.fz == 2 ? -1 : 0, dz1 = T.fz == 2 ? 1 : 0;
   const int dy0 = T.fy == 2 ? -1 : 0, dy1 = T.fy == 2 ? 1 : 0;
   const int dx0 = T.fx == 2 ? -1 : 0, dx1 = T.fx == 2 ? 1 : 0;
@@ -465,28 +454,24 @@ __global__ void k_mg_restrict(Transfer T, const float* __restrict__ tf, const ui
         const int i = T.fx * I + di;
         if (i < 0 || i >= T.NXf) continue;
         const float w = (dk ? 0.5f : 1.f) * (dj ? 0.5f : 1.f) * (di ? 0.5f : 1.f);
-        const int n = (k * T.NYf + j) * T.NXf + i;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const float4 v = __ldg(reinterpret_cast<const float4*>(tf + r * vsf) + n);
-          acc[r][0] += w * v.x; acc[r][1] += w * v.y; acc[r][2] += w * v.z;
-        }
+        const float4 v = __ldg(src + (k * T.NYf + j) * T.NXf + i);
+        acc[0] += w * v.x; acc[1] += w * v.y; acc[2] += w * v.z;
       }
     }
   }
   const uint8_t fx = fixc[N];
-#pragma unroll
-  for (int r = 0; r < R; ++r)
-    reinterpret_cast<float4*>(rc + r * vsc)[N] = make_float4((fx & 1) ? 0.f : acc[r][0], (fx & 2) ? 0.f : acc[r][1],
-                                                             (fx & 4) ? 0.f : acc[r][2], 0.f);
+  reinterpret_cast<float4*>(rc + r * vsc)[N] =
+      make_float4((fx & 1) ? 0.f : acc[0], (fx & 2) ? 0.f : acc[1], (fx & 4) ? 0.f : acc[2], 0.f);
 }
 
-// e_f += P e_c (masked by the fine fixed bits)
-template <int R>
-__global__ void k_mg_prolong(Transfer T, const float* __restrict__ ec, const uint8_t* __restrict__ fixf, float* ef) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+// e_f += P e_c (masked by the fine fixed bits); one thread per (fine node,
+// right-hand side)
+__global__ void k_mg_prolong(Transfer T, int R, const float* __restrict__ ec, const uint8_t* __restrict__ fixf,
+                             float* ef) {
   const int NNf = T.NXf * T.NYf * T.NZf;
-  if (n >= NNf) return;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)NNf * R) return;
+  const int n = int(t % NNf), r = int(t / NNf);
   int i, j, k;
   node_ijk(n, T.NXf, T.NYf, i, j, k);
   const long long vsf = (long long)NNf * 4, vsc = (long long)T.NXc * T.NYc * T.NZc * 4;
@@ -500,55 +485,47 @@ __global__ void k_mg_prolong(Transfer T, const float* __restrict__ ec, const uin
   axis(T.fx, i, Ix, wx, cx);
   axis(T.fy, j, Iy, wy, cy);
   axis(T.fz, k, Iz, wz, cz);
-  float acc[R][3];
-#pragma unroll
-  for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.f;
+  const float4* src = reinterpret_cast<const float4*>(ec + r * vsc);
+  float acc[3] = {0.f, 0.f, 0.f};
   for (int c = 0; c < cz; ++c)
     for (int b = 0; b < cy; ++b)
       for (int a = 0; a < cx; ++a) {
         const float w = wx[a] * wy[b] * wz[c];
-        const int N = (Iz[c] * T.NYc + Iy[b]) * T.NXc + Ix[a];
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const float4 v = __ldg(reinterpret_cast<const float4*>(ec + r * vsc) + N);
-          acc[r][0] += w * v.x; acc[r][1] += w * v.y; acc[r][2] += w * v.z;
-        }
+        const float4 v = __ldg(src + (Iz[c] * T.NYc + Iy[b]) * T.NXc + Ix[a]);
+        acc[0] += w * v.x; acc[1] += w * v.y; acc[2] += w * v.z;
       }
   const uint8_t fx = fixf[n];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    float4 o = reinterpret_cast<float4*>(ef + r * vsf)[n];
-    if (!(fx & 1)) o.x += acc[r][0];
-    if (!(fx & 2)) o.y += acc[r][1];
-    if (!(fx & 4)) o.z += acc[r][2];
-    reinterpret_cast<float4*>(ef + r * vsf)[n] = o;
-  }
+  float4 o = reinterpret_cast<float4*>(ef + r * vsf)[n];
+  if (!(fx & 1)) o.x += acc[0];
+  if (!(fx & 2)) o.y += acc[1];
+  if (!(fx & 4)) o.z += acc[2];
+  reinterpret_cast<float4*>(ef + r * vsf)[n] = o;
 }
 
-// coarsest: e = Ainv r (one CTA, n <= 3 * kCoarseNodes)
-__global__ void __launch_bounds__(256) k_mg_coarse_solve(int NN, int R, const double* __restrict__ Ainv,
+// coarsest: e = Ainv r, one CTA per right-hand side (n <= 3 * kCoarseNodes).
+// Ainv is symmetric, so row i is read as column i: consecutive threads read
+// consecutive addresses.
+__global__ void __launch_bounds__(256) k_mg_coarse_solve(int NN, const double* __restrict__ Ainv,
                                                          const float* __restrict__ r, float* e) {
-  __shared__ double sr[8][3 * kCoarseNodes];
+  __shared__ double sr[3 * kCoarseNodes];
   const int n = 3 * NN;
-  for (int w = threadIdx.x; w < R * n; w += blockDim.x) {
-    const int rr = w / n, i = w % n;
-    sr[rr][i] = double(r[(size_t)rr * NN * 4 + (i / 3) * 4 + i % 3]);
-  }
+  const float* rr = r + (size_t)blockIdx.x * NN * 4;
+  float* er = e + (size_t)blockIdx.x * NN * 4;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sr[i] = double(rr[(i / 3) * 4 + i % 3]);
   __syncthreads();
-  for (int w = threadIdx.x; w < R * n; w += blockDim.x) {
-    const int rr = w / n, i = w % n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double s = 0.0;
-    for (int j = 0; j < n; ++j) s = fma(Ainv[(size_t)i * n + j], sr[rr][j], s);
-    e[(size_t)rr * NN * 4 + (i / 3) * 4 + i % 3] = float(s);
+    for (int j = 0; j < n; ++j) s = fma(Ainv[(size_t)j * n + i], sr[j], s);
+    er[(i / 3) * 4 + i % 3] = float(s);
   }
-  for (int w = threadIdx.x; w < R * NN; w += blockDim.x) e[(size_t)(w / NN) * NN * 4 + (w % NN) * 4 + 3] = 0.f;
+  for (int i = threadIdx.x; i < NN; i += blockDim.x) er[i * 4 + 3] = 0.f;
 }
 
 // ---------------------------------------------------------------------------
 // host: hierarchy, setup, V-cycle
 // ---------------------------------------------------------------------------
 static LevelView view(const MGLevel& L) {
-  return LevelView{L.nx, L.ny, L.nz, L.NX, L.NY, L.NZ, L.NN, L.Ae, L.dinv, L.fix};
+  return LevelView{L.nx, L.ny, L.nz, L.NX, L.NY, L.NZ, L.NN, L.St, L.dinv, L.fix};
 }
 static Transfer transfer(const MGLevel& f, const MGLevel& c) {
   return Transfer{f.NX, f.NY, f.NZ, c.NX, c.NY, c.NZ, c.fx, c.fy, c.fz};
@@ -593,6 +570,7 @@ int mg_create(Ctx& c, int maxR) {
       al(&L.Ae, (size_t)L.NE * 576);
       al(&L.dinv, (size_t)L.NN * 4);
       al(&L.fix, (size_t)L.NN);
+      if (k < mg->nlev - 1) al(&L.St, (size_t)L.NN * 243);
     } else {
       L.dinv = c.dinvK32;
       L.fix = c.fix;
@@ -616,7 +594,7 @@ void mg_destroy(Ctx& c) {
   if (!mg) return;
   for (int k = 0; k < mg->nlev; ++k) {
     MGLevel& L = mg->L[k];
-    if (k > 0) { cudaFree(L.Ae); cudaFree(L.dinv); cudaFree(L.fix); }
+    if (k > 0) { cudaFree(L.Ae); cudaFree(L.dinv); cudaFree(L.fix); if (L.St) cudaFree(L.St); }
     cudaFree(L.r); cudaFree(L.e); cudaFree(L.e2); cudaFree(L.t);
   }
   for (auto& g : mg->gexec)
@@ -646,6 +624,10 @@ int mg_setup(Ctx& c, cudaStream_t s) {
     count_launch();
     k_mg_diag<<<ceil_div(C.NN, 128), 128, 0, s>>>(C.nx, C.ny, C.nz, C.Ae, C.dinv, C.fix);
     count_launch();
+    if (C.St) {
+      k_mg_stencil<<<int((27LL * C.NN + 255) / 256), 256, 0, s>>>(C.nx, C.ny, C.nz, C.Ae, C.St);
+      count_launch();
+    }
   }
   const MGLevel& L = mg->L[mg->nlev - 1];
   k_mg_coarse_setup<<<1, 256, 0, s>>>(L.nx, L.ny, L.nz, mg->nlev > 1 ? L.Ae : nullptr, c.fK64, c.Ke64, L.fix, mg->A,
@@ -664,8 +646,7 @@ int mg_setup(Ctx& c, cudaStream_t s) {
         k_mg_scale_dinv<<<ceil_div(V.NN, 256), 256, 0, s>>>(V.NN, V.dinv, y);
         count_launch();
       } else {
-        k_mgc_op<1><<<ceil_div(V.NN, 128), 128, 0, s>>>(view(V), x, nullptr, y, nullptr, 2);
-        count_launch();
+        launch_mgs_op(view(V), 1, x, nullptr, y, nullptr, 2, s);
       }
       std::swap(x, y);
     }
@@ -699,18 +680,18 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
     count_launch();
     for (int sw = 1; sw < mg->nu; ++sw) {
       if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
-      else { k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1); count_launch(); }
+      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], om, 1, s);
       std::swap(cur[k], alt[k]);
     }
     if (k == 0) { if (launch_matvec(c, 0, false, cur[k], L.t, R, L.r, s)) return -2; }
-    else { k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, L.t, nullptr, 0); count_launch(); }
+    else launch_mgs_op(view(L), R, cur[k], L.r, L.t, nullptr, 0, s);
     MGLevel& C = mg->L[k + 1];
-    k_mg_restrict<R><<<grid1(C.NN), 128, 0, s>>>(transfer(L, C), L.t, C.fix, C.r);
+    k_mg_restrict<<<grid1(C.NN * R), 128, 0, s>>>(transfer(L, C), R, L.t, C.fix, C.r);
     count_launch();
   }
   {
     MGLevel& L = mg->L[nl - 1];
-    k_mg_coarse_solve<<<1, 256, 0, s>>>(L.NN, R, mg->Ainv, L.r, L.e);
+    k_mg_coarse_solve<<<R, 256, 0, s>>>(L.NN, mg->Ainv, L.r, L.e);
     count_launch();
     cur[nl - 1] = L.e;
   }
@@ -718,12 +699,12 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
   for (int k = nl - 2; k >= 0; --k) {
     MGLevel& L = mg->L[k];
     MGLevel& C = mg->L[k + 1];
-    k_mg_prolong<R><<<grid1(L.NN), 128, 0, s>>>(transfer(L, C), cur[k + 1], L.fix, cur[k]);
+    k_mg_prolong<<<grid1(L.NN * R), 128, 0, s>>>(transfer(L, C), R, cur[k + 1], L.fix, cur[k]);
     count_launch();
     const float* om = mg->omega + k;
     for (int sw = 0; sw < mg->nu; ++sw) {
       if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
-      else { k_mgc_op<R><<<grid1(L.NN), 128, 0, s>>>(view(L), cur[k], L.r, alt[k], om, 1); count_launch(); }
+      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], om, 1, s);
       std::swap(cur[k], alt[k]);
     }
   }
@@ -734,7 +715,7 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
 int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
   if (c.mg->nlev == 1) {
     MGLevel& L = c.mg->L[0];
-    k_mg_coarse_solve<<<1, 256, 0, s>>>(L.NN, R, c.mg->Ainv, L.r, L.e);
+    k_mg_coarse_solve<<<R, 256, 0, s>>>(L.NN, c.mg->Ainv, L.r, L.e);
     count_launch();
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
   }

@@ -66,6 +66,7 @@ struct Ctx {
   BarrierState* bar = nullptr;
   int* status = nullptr;       // [16] solver status words
   double* scal = nullptr;      // [256] solver scalars
+  unsigned* counters = nullptr; // [16] last-block reduction counters (each kernel resets its own)
 
   // PCG workspace
   float* pw32 = nullptr;       // 10 node4 blocks of max_rhs vectors (FP32)

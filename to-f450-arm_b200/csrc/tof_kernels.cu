@@ -279,87 +279,117 @@ void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long lo
 
 // ---------------------------------------------------------------------------
 // Gram matrix G = A^T B of two blocks of node4 vectors (na, nb <= 24) with
-// FP64 accumulation.  Stage 1: each CTA reduces a contiguous range of node
-// chunks into a partial matrix; stage 2 sums the partials in block order
-// (deterministic).
+// FP64 accumulation.
+//
+// Stage 1 (k_gram_partial): each CTA stages a chunk of kGramChunk nodes of all
+// na + nb vectors in shared memory (converted to FP64, one padded row per
+// vector) and every warp accumulates the full 24 x 24 product over its own
+// nodes of the chunk: lane (rg, cg) = (lane & 7, lane >> 3) owns rows
+// 3rg..3rg+2 and columns 6cg..6cg+5, i.e. 9 shared loads per 18 FMAs.  The
+// row pitch kGramLd (98 doubles: consecutive rows start 4 banks apart) makes
+// both the 8 distinct row reads and the 4 distinct column reads of a warp
+// conflict-free.  The 8 warps' tiles are summed in a fixed order into one
+// partial per CTA.
+// Stage 2 (k_gram_reduce): one warp per output sums the CTA partials in a
+// fixed lane-strided order (deterministic).
 // ---------------------------------------------------------------------------
 constexpr int kGramThreads = 256;
-constexpr int kGramMaxPerThread = 3;   // 24*24 = 576 <= 3*256 - 192
+constexpr int kGramChunk = 24;                       // nodes per staged chunk
+constexpr int kGramLd = 4 * kGramChunk + 2;          // doubles per staged vector row
 
-template <typename T, int CH>
+template <typename T>
 __global__ void __launch_bounds__(kGramThreads) k_gram_partial(int NN, const T* __restrict__ A, int na,
                                                               const T* __restrict__ B, int nb, long long vstride,
                                                               double* part) {
   using V4 = typename Vec4<T>::type;
-  __shared__ V4 sA[24 * CH];
-  __shared__ V4 sB[24 * CH];
-  const int npair = na * nb;
-  double acc[kGramMaxPerThread] = {0, 0, 0};
-  const int nchunks = (NN + CH - 1) / CH;
-  const int per = (nchunks + gridDim.x - 1) / gridDim.x;
-  const int c0 = blockIdx.x * per, c1 = min(nchunks, c0 + per);
-  for (int ch = c0; ch < c1; ++ch) {
-    const int n0 = ch * CH;
-    const int cnt = min(CH, NN - n0);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < na * CH; idx += blockDim.x) {
-      const int v = idx / CH, q = idx % CH;
-      V4 z{};
-      sA[idx] = q < cnt ? reinterpret_cast<const V4*>(A + v * vstride)[n0 + q] : z;
-    }
-    for (int idx = threadIdx.x; idx < nb * CH; idx += blockDim.x) {
-      const int v = idx / CH, q = idx % CH;
-      V4 z{};
-      sB[idx] = q < cnt ? reinterpret_cast<const V4*>(B + v * vstride)[n0 + q] : z;
-    }
-    __syncthreads();
+  __shared__ __align__(16) double sm[48 * kGramLd];   // rows 0..23: A, 24..47: B
+  static_assert(48 * kGramLd >= 8 * 576, "reduction scratch");
+  double* sA = sm;
+  double* sB = sm + 24 * kGramLd;
+  for (int i = threadIdx.x; i < 48 * kGramLd; i += blockDim.x) sm[i] = 0.0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rg = lane & 7, cg = lane >> 3;
+  double acc[3][6];
 #pragma unroll
-    for (int t = 0; t < kGramMaxPerThread; ++t) {
-      const int p = threadIdx.x + t * kGramThreads;
-      if (p < npair) {
-        const int ia = p / nb, ib = p % nb;
-        const V4* a = sA + ia * CH;
-        const V4* b = sB + ib * CH;
-        double s = 0.0;
-        for (int q = 0; q < cnt; ++q) {
-          const V4 x = a[q], y = b[q];
-          s = fma(double(x.x), double(y.x), s);
-          s = fma(double(x.y), double(y.y), s);
-          s = fma(double(x.z), double(y.z), s);
-        }
-        acc[t] += s;
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) acc[i][j] = 0.0;
+  const int nchunks = (NN + kGramChunk - 1) / kGramChunk;
+  const int nstage = (na + nb) * kGramChunk;
+  for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int n0 = ch * kGramChunk;
+    const int cnt = min(kGramChunk, NN - n0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nstage; idx += blockDim.x) {
+      const int v = idx / kGramChunk, q = idx % kGramChunk;
+      if (q >= cnt) continue;
+      const bool isA = v < na;
+      const T* src = isA ? A + v * vstride : B + (v - na) * vstride;
+      const V4 x = reinterpret_cast<const V4*>(src)[n0 + q];
+      double* d = (isA ? sA + v * kGramLd : sB + (v - na) * kGramLd) + 4 * q;
+      reinterpret_cast<double2*>(d)[0] = make_double2(double(x.x), double(x.y));
+      reinterpret_cast<double2*>(d)[1] = make_double2(double(x.z), 0.0);
+    }
+    __syncthreads();
+    const double* pa = sA + 3 * rg * kGramLd;
+    const double* pb = sB + 6 * cg * kGramLd;
+    for (int q = w; q < cnt; q += kGramThreads / 32) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int o = 4 * q + c;
+        double a[3], b[6];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) a[i] = pa[i * kGramLd + o];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) b[j] = pb[j * kGramLd + o];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 6; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
       }
     }
   }
+  // CTA reduction of the 8 warp tiles (fixed order)
+  __syncthreads();
+  double* red = sm;
 #pragma unroll
-  for (int t = 0; t < kGramMaxPerThread; ++t) {
-    const int p = threadIdx.x + t * kGramThreads;
-    if (p < npair) part[(size_t)blockIdx.x * 576 + p] = acc[t];
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) red[w * 576 + (3 * rg + i) * 24 + 6 * cg + j] = acc[i][j];
+  __syncthreads();
+  for (int p = threadIdx.x; p < na * nb; p += blockDim.x) {
+    const int r = p / nb, col = p % nb;
+    double sum = 0.0;
+#pragma unroll
+    for (int k = 0; k < kGramThreads / 32; ++k) sum += red[k * 576 + r * 24 + col];
+    part[(size_t)blockIdx.x * 576 + p] = sum;
   }
 }
 
-__global__ void k_gram_reduce(int nblocks, int npair, const double* __restrict__ part, double* G) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_gram_reduce(int nblocks, int npair, const double* __restrict__ part,
+                                                     double* G) {
+  const int p = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
   if (p >= npair) return;
   double s = 0.0;
-  for (int b = 0; b < nblocks; ++b) s += part[(size_t)b * 576 + p];
-  G[p] = s;
+  for (int b = lane; b < nblocks; b += 32) s += part[(size_t)b * 576 + p];
+  s = warp_sum(s);
+  if (lane == 0) G[p] = s;
 }
 
 void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s) {
-  const int CH = f64 ? 16 : 32;
-  const int nchunks = ceil_div(c.g.NN, CH);
+  const int nchunks = ceil_div(c.g.NN, kGramChunk);
   int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
   if (blocks < 1) blocks = 1;
   const long long vs = (long long)c.g.NN * 4;
   if (f64)
-    k_gram_partial<double, 16><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, na, (const double*)B, nb,
-                                                               vs, c.gram_part);
+    k_gram_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, na, (const double*)B, nb, vs,
+                                                          c.gram_part);
   else
-    k_gram_partial<float, 32><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, na, (const float*)B, nb,
-                                                              vs, c.gram_part);
+    k_gram_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, na, (const float*)B, nb, vs,
+                                                         c.gram_part);
   count_launch();
-  k_gram_reduce<<<ceil_div(na * nb, 128), 128, 0, s>>>(blocks, na * nb, c.gram_part, G);
+  k_gram_reduce<<<ceil_div(na * nb, 8), 256, 0, s>>>(blocks, na * nb, c.gram_part, G);
   count_launch();
 }
 

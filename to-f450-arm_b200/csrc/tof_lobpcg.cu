@@ -32,9 +32,10 @@ constexpr int kMaxBasis = 24;
 template <typename T>
 __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs, const T* __restrict__ KX,
                                                    const T* __restrict__ MX, const double* __restrict__ theta,
-                                                   const T* __restrict__ dinv, T* W, double* part) {
+                                                   const T* __restrict__ dinv, T* W, double* part,
+                                                   unsigned* counter, double* out) {
   using V4 = typename Vec4<T>::type;
-  __shared__ double red[2 * 8 * 32];
+  __shared__ double red[16 * 32];
   double v[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) v[k] = 0.0;
@@ -56,40 +57,40 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
       reinterpret_cast<V4*>(W)[o] = w;
     }
   }
-  block_sum<16>(v, red);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < 16; ++k) part[(size_t)blockIdx.x * 16 + k] = v[k];
-}
-
-__global__ void k_lob_resid_reduce(int nblk, const double* __restrict__ part, double* out) {
-  const int k = threadIdx.x;
-  if (k >= 16) return;
-  double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[(size_t)b * 16 + k];
-  out[k] = s;
+  double tot[16];
+  if (last_block<16>(v, part, counter, red, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) out[k] = tot[k];
+  }
 }
 
 // ---------------------------------------------------------------------------
-// One-warp parallel cyclic Jacobi eigensolver for a symmetric n x n (n <= 24)
+// CTA-parallel cyclic Jacobi eigensolver for a symmetric n x n (n <= 24)
 // matrix held in shared memory.  Round-robin ordering applies n/2 disjoint
-// rotations per step (rows, then columns, then the eigenvector matrix).
+// rotations per step (rows, then columns and the eigenvector matrix), each
+// element update by its own thread.  Stops when the off-diagonal Frobenius
+// norm is below 1e-13 of the total (eigenvalue errors ~1e-26 relative).
 // Rotation: Golub & Van Loan, Matrix Computations, Alg. 8.4.1 (sym.schur2).
 // ---------------------------------------------------------------------------
 constexpr int LDA = kMaxBasis + 1;
+constexpr int kEigThreads = 128;
 
-__device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane) {
+__device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
+  const int tid = threadIdx.x, nt = blockDim.x;
   const int np = n + (n & 1);
-  for (int w = lane; w < np * np; w += 32) {
-    const int i = w / np, j = w % np;
-    V[i][j] = (i == j) ? 1.0 : 0.0;
-    if (i >= n || j >= n) A[i][j] = (i == j) ? 0.0 : 0.0;
-  }
-  __syncwarp();
   __shared__ double cs_s[kMaxBasis / 2], sn_s[kMaxBasis / 2];
   __shared__ int P_s[kMaxBasis / 2], Q_s[kMaxBasis / 2];
-  for (int sweep = 0; sweep < 40; ++sweep) {
+  __shared__ double red[2][kEigThreads / 32];
+  __shared__ int s_go;
+  for (int w = tid; w < np * np; w += nt) {
+    const int i = w / np, j = w % np;
+    V[i][j] = (i == j) ? 1.0 : 0.0;
+    if (i >= n || j >= n) A[i][j] = 0.0;
+  }
+  __syncthreads();
+  for (int sweep = 0; sweep < 30; ++sweep) {
     double off = 0.0, tot = 0.0;
-    for (int w = lane; w < n * n; w += 32) {
+    for (int w = tid; w < n * n; w += nt) {
       const int i = w / n, j = w % n;
       const double a = A[i][j];
       tot += a * a;
@@ -97,10 +98,18 @@ __device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane)
     }
     off = warp_sum(off);
     tot = warp_sum(tot);
-    if (!(off > 1e-30 * tot) || np < 2) break;
+    if ((tid & 31) == 0) { red[0][tid >> 5] = off; red[1][tid >> 5] = tot; }
+    __syncthreads();
+    if (tid == 0) {
+      double o = 0.0, t = 0.0;
+      for (int w = 0; w < (nt + 31) / 32; ++w) { o += red[0][w]; t += red[1][w]; }
+      s_go = (o > 1e-26 * t) && np >= 2;
+    }
+    __syncthreads();
+    if (!s_go) break;
     for (int r = 0; r < np - 1; ++r) {
-      if (lane < np / 2) {
-        const int k = lane;
+      if (tid < np / 2) {
+        const int k = tid;
         auto pos = [&](int q) { return q == 0 ? 0 : 1 + ((q - 1 + r) % (np - 1)); };
         int p = pos(k), q = pos(np - 1 - k);
         if (p > q) { const int t = p; p = q; q = t; }
@@ -116,10 +125,9 @@ __device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane)
         }
         P_s[k] = p; Q_s[k] = q; cs_s[k] = c; sn_s[k] = s;
       }
-      __syncwarp();
+      __syncthreads();
       const int npair = np / 2;
-      // rows: A <- J^T A
-      for (int w = lane; w < npair * np; w += 32) {
+      for (int w = tid; w < npair * np; w += nt) {       // rows: A <- J^T A
         const int k = w / np, j = w % np;
         const int p = P_s[k], q = Q_s[k];
         const double c = cs_s[k], s = sn_s[k];
@@ -127,9 +135,8 @@ __device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane)
         A[p][j] = c * ap - s * aq;
         A[q][j] = s * ap + c * aq;
       }
-      __syncwarp();
-      // columns: A <- A J ; V <- V J
-      for (int w = lane; w < npair * np; w += 32) {
+      __syncthreads();
+      for (int w = tid; w < npair * np; w += nt) {       // columns: A <- A J ; V <- V J
         const int k = w / np, j = w % np;
         const int p = P_s[k], q = Q_s[k];
         const double c = cs_s[k], s = sn_s[k];
@@ -140,7 +147,7 @@ __device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane)
         V[j][p] = c * vp - s * vq;
         V[j][q] = s * vp + c * vq;
       }
-      __syncwarp();
+      __syncthreads();
     }
   }
 }
@@ -150,27 +157,27 @@ __device__ void warp_jacobi(double (*A)[LDA], double (*V)[LDA], int n, int lane)
 // eigenvalue below drop_tol * max are discarded (a near-dependent basis), and
 // the standard problem is solved in the remaining orthonormal basis.
 // Outputs: C (n x m, row-major), theta (m), info[0] = kept rank (or -1).
-__global__ void k_small_eig(int n, int m, const double* __restrict__ GK, const double* __restrict__ GM,
-                            double drop_tol, double* C, double* theta, int* info) {
+__global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const double* __restrict__ GK,
+                                                          const double* __restrict__ GM, double drop_tol, double* C,
+                                                          double* theta, int* info) {
   __shared__ double A[kMaxBasis][LDA], B[kMaxBasis][LDA], V[kMaxBasis][LDA], Z[kMaxBasis][LDA];
   __shared__ double D[kMaxBasis], ev[kMaxBasis];
   __shared__ int keep[kMaxBasis], order[kMaxBasis];
   __shared__ int kr;
-  const int lane = threadIdx.x;
-  for (int w = lane; w < n; w += 32) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int w = tid; w < n; w += nt) {
     const double b = GM[w * n + w];
     D[w] = b > 0.0 ? 1.0 / sqrt(b) : 0.0;
   }
-  __syncwarp();
-  for (int w = lane; w < n * n; w += 32) {
+  __syncthreads();
+  for (int w = tid; w < n * n; w += nt) {
     const int i = w / n, j = w % n;
     A[i][j] = 0.5 * (GK[i * n + j] + GK[j * n + i]) * D[i] * D[j];
     B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
   }
-  __syncwarp();
-  warp_jacobi(B, V, n, lane);
-  // kept directions of the basis
-  if (lane == 0) {
+  __syncthreads();
+  cta_jacobi(B, V, n);
+  if (tid == 0) {
     double bmax = 0.0;
     for (int i = 0; i < n; ++i) bmax = fmax(bmax, B[i][i]);
     int k = 0;
@@ -178,47 +185,44 @@ __global__ void k_small_eig(int n, int m, const double* __restrict__ GK, const d
       if (D[i] > 0.0 && B[i][i] > drop_tol * bmax) keep[k++] = i;
     kr = k;
   }
-  __syncwarp();
+  __syncthreads();
   const int K = kr;
-  // Z = V[:, keep] / sqrt(lambda)
-  for (int w = lane; w < n * K; w += 32) {
+  for (int w = tid; w < n * K; w += nt) {                 // Z = V[:, keep] / sqrt(lambda)
     const int i = w / K, a = w % K;
     Z[i][a] = V[i][keep[a]] / sqrt(B[keep[a]][keep[a]]);
   }
-  __syncwarp();
-  // V <- A Z  (n x K), then B <- Z^T V (K x K)
-  for (int w = lane; w < n * K; w += 32) {
+  __syncthreads();
+  for (int w = tid; w < n * K; w += nt) {                 // V <- A Z
     const int i = w / K, a = w % K;
     double s = 0.0;
     for (int j = 0; j < n; ++j) s = fma(A[i][j], Z[j][a], s);
     V[i][a] = s;
   }
-  __syncwarp();
-  for (int w = lane; w < K * K; w += 32) {
+  __syncthreads();
+  for (int w = tid; w < K * K; w += nt) {                 // B <- Z^T V
     const int a = w / K, b = w % K;
     double s = 0.0;
     for (int j = 0; j < n; ++j) s = fma(Z[j][a], V[j][b], s);
     B[a][b] = s;
   }
-  __syncwarp();
-  for (int w = lane; w < K * K; w += 32) {
+  __syncthreads();
+  for (int w = tid; w < K * K; w += nt) {
     const int a = w / K, b = w % K;
     A[a][b] = 0.5 * (B[a][b] + B[b][a]);
   }
-  __syncwarp();
-  warp_jacobi(A, V, K, lane);
-  if (lane == 0) {
+  __syncthreads();
+  cta_jacobi(A, V, K);
+  if (tid == 0) {
     for (int i = 0; i < K; ++i) { ev[i] = A[i][i]; order[i] = i; }
     for (int i = 0; i < K; ++i)
       for (int j = i + 1; j < K; ++j)
         if (ev[order[j]] < ev[order[i]]) { const int t = order[i]; order[i] = order[j]; order[j] = t; }
     info[0] = K >= m ? K : -1;
   }
-  __syncwarp();
+  __syncthreads();
   if (K < m) return;
-  for (int w = lane; w < m; w += 32) theta[w] = ev[order[w]];
-  // C = D Z U[:, order[:m]]
-  for (int w = lane; w < n * m; w += 32) {
+  for (int w = tid; w < m; w += nt) theta[w] = ev[order[w]];
+  for (int w = tid; w < n * m; w += nt) {                 // C = D Z U[:, order[:m]]
     const int i = w / m, k = w % m;
     double s = 0.0;
     for (int a = 0; a < K; ++a) s = fma(Z[i][a], V[a][order[k]], s);
@@ -226,45 +230,54 @@ __global__ void k_small_eig(int n, int m, const double* __restrict__ GK, const d
   }
 }
 
+
 // ---------------------------------------------------------------------------
 // block update: Xn = S C, Pn = S[:, nb:] C[nb:, :] for S, KS, MS
 // ---------------------------------------------------------------------------
+// One thread per (node, block in {S, KS, MS}, component): ncols inputs, 2 nb
+// outputs, all in registers.  The 4th (padding) component of the outputs is
+// never written and stays zero.
 template <typename T>
 __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, long long vs,
                                                     const T* __restrict__ S, const T* __restrict__ KS,
                                                     const T* __restrict__ MS, const double* __restrict__ C,
                                                     T* S2, T* KS2, T* MS2) {
-  using V4 = typename Vec4<T>::type;
   __shared__ T sC[kMaxBasis * 8];
   for (int i = threadIdx.x; i < ncols * nb; i += blockDim.x) sC[i] = T(C[i]);
   __syncthreads();
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= NN) return;
-  const T* src[3] = {S, KS, MS};
-  T* dst[3] = {S2, KS2, MS2};
-#pragma unroll 1
-  for (int b = 0; b < 3; ++b) {
-    V4 in[kMaxBasis];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 9LL * NN) return;
+  const int n = int(t % NN);
+  const int bc = int(t / NN);
+  const int b = bc / 3, c = bc % 3;
+  const T* src = b == 0 ? S : b == 1 ? KS : MS;
+  T* dst = b == 0 ? S2 : b == 1 ? KS2 : MS2;
+  const size_t o = 4 * (size_t)n + c;
+  T in[kMaxBasis];
 #pragma unroll
-    for (int j = 0; j < kMaxBasis; ++j)
-      if (j < ncols) in[j] = reinterpret_cast<const V4*>(src[b])[j * vs / 4 + n];
+  for (int j = 0; j < kMaxBasis; ++j) in[j] = j < ncols ? src[j * vs + o] : T(0);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      if (k >= nb) break;
-      V4 x{}, p{};
+  for (int k = 0; k < 8; ++k) {
+    if (k >= nb) break;
+    T x = T(0), p = T(0);
 #pragma unroll
-      for (int j = 0; j < kMaxBasis; ++j) {
-        if (j < ncols) {
-          const T c = sC[j * nb + k];
-          x.x = fma(c, in[j].x, x.x); x.y = fma(c, in[j].y, x.y); x.z = fma(c, in[j].z, x.z);
-          if (j >= nb) { p.x = fma(c, in[j].x, p.x); p.y = fma(c, in[j].y, p.y); p.z = fma(c, in[j].z, p.z); }
-        }
+    for (int j = 0; j < kMaxBasis; ++j) {
+      if (j < ncols) {
+        const T cf = sC[j * nb + k];
+        x = fma(cf, in[j], x);
+        if (j >= nb) p = fma(cf, in[j], p);
       }
-      x.w = T(0); p.w = T(0);
-      reinterpret_cast<V4*>(dst[b])[k * vs / 4 + n] = x;
-      reinterpret_cast<V4*>(dst[b])[(2 * nb + k) * vs / 4 + n] = p;
     }
+    dst[k * vs + o] = x;
+    dst[(2 * nb + k) * vs + o] = p;
   }
+}
+
+template <typename T>
+static void launch_lob_update(int NN, int nb, int ncols, long long vs, const T* S, const T* KS, const T* MS,
+                              const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s) {
+  k_lob_update<T><<<int((9LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, vs, S, KS, MS, C, S2, KS2, MS2);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -287,7 +300,7 @@ static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s) {
   double* C = c.gram + 2 * 576;
   double* th = c.gram + 3 * 576;
   int* info = c.status + 8;
-  k_small_eig<<<1, 32, 0, s>>>(n, m, GK, GM, drop, C, th, info);
+  k_small_eig<<<1, kEigThreads, 0, s>>>(n, m, GK, GM, drop, C, th, info);
   count_launch();
   return 0;
 }
@@ -329,9 +342,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   launch_gram(c, f64, B.S[cur], nb, B.KS[cur], nb, GK, s);
   launch_gram(c, f64, B.S[cur], nb, B.MS[cur], nb, GM, s);
   lob_small_eig(c, nb, nb, drop, s);
-  k_lob_update<T><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, nb, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
-                                                     (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1]);
-  count_launch();
+  launch_lob_update<T>(NN, nb, nb, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
+                       (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
   cur ^= 1;
   int it = 0;
   double hr[16];
@@ -346,9 +358,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     T* W = vec<T>(B.S[cur], nb, vs);
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
-    k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, W, c.gram_part);
-    count_launch();
-    k_lob_resid_reduce<<<1, 32, 0, s>>>(rblocks, c.gram_part, rn);
+    k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, W, c.gram_part,
+                                           c.counters, rn);
     count_launch();
     cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
@@ -392,10 +403,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     launch_gram(c, f64, B.S[cur], ncols, B.MS[cur], ncols, GM, s);
     lob_small_eig(c, ncols, nb, drop, s);
     cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
-    k_lob_update<T><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, ncols, vs, (T*)B.S[cur], (T*)B.KS[cur],
-                                                       (T*)B.MS[cur], C, (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1],
-                                                       (T*)B.MS[cur ^ 1]);
-    count_launch();
+    launch_lob_update<T>(NN, nb, ncols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
+                         (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
     cur ^= 1;
     (void)X;
   }
@@ -417,10 +426,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     // reuse the update kernel: S = X6 (ncols = nb), P part unused -> KS2/MS2 scratch
     double* scratch = c.lw64 + 3LL * c.max_modes * vs;   // FP64 LOBPCG area (free in mixed mode)
     if (f64) scratch = (double*)B.S[cur ^ 1];
-    k_lob_update<double><<<ceil_div(NN, 128), 128, 0, s>>>(NN, nb, nb, vs, X6, KX6, MX6, C, scratch,
-                                                            scratch + 3LL * c.max_modes * vs,
-                                                            scratch + 6LL * c.max_modes * vs);
-    count_launch();
+    launch_lob_update<double>(NN, nb, nb, vs, X6, KX6, MX6, C, scratch, scratch + 3LL * c.max_modes * vs,
+                              scratch + 6LL * c.max_modes * vs, s);
     cudaMemcpyAsync(out, scratch, sizeof(double) * nmodes * vs, cudaMemcpyDeviceToDevice, s);
   }
   cudaMemcpyAsync(hth, th, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
