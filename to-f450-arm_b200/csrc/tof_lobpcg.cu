@@ -24,6 +24,10 @@
 namespace tof {
 
 constexpr int kMaxBasis = 24;
+#ifndef TOF_LOB_REFRESH
+#define TOF_LOB_REFRESH 10
+#endif
+constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M products
 
 // ---------------------------------------------------------------------------
 // residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, and per-CTA
@@ -65,48 +69,37 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
 }
 
 // ---------------------------------------------------------------------------
-// CTA-parallel cyclic Jacobi eigensolver for a symmetric n x n (n <= 24)
-// matrix held in shared memory.  Round-robin ordering applies n/2 disjoint
-// rotations per step (rows, then columns and the eigenvector matrix), each
-// element update by its own thread.  Stops when the off-diagonal Frobenius
-// norm is below 1e-13 of the total (eigenvalue errors ~1e-26 relative).
+// CTA-parallel cyclic Jacobi eigensolver for a symmetric positive
+// semi-definite n x n (n <= 24) matrix held in shared memory.  Round-robin
+// ordering applies n/2 disjoint rotations per step (rows, then columns and
+// the eigenvector matrix), each element update by its own thread.  A pair
+// (p, q) is rotated only while |a_pq| > kJacobiRel * sqrt(a_pp a_qq); the
+// iteration stops after a sweep without rotations.  That relative test
+// (Demmel & Veselic, SIAM J. Matrix Anal. Appl. 13 (1992)) keeps the small
+// eigenvalues and their eigenvectors accurate to working precision relative
+// to themselves, which the Rayleigh-Ritz step needs: its projected matrices
+// span the whole spectrum of K, and the wanted pairs sit at the bottom.
 // Rotation: Golub & Van Loan, Matrix Computations, Alg. 8.4.1 (sym.schur2).
 // ---------------------------------------------------------------------------
 constexpr int LDA = kMaxBasis + 1;
 constexpr int kEigThreads = 128;
+constexpr double kJacobiRel = 1e-15;
+constexpr int kJacobiSweeps = 40;
 
 __device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const int np = n + (n & 1);
   __shared__ double cs_s[kMaxBasis / 2], sn_s[kMaxBasis / 2];
   __shared__ int P_s[kMaxBasis / 2], Q_s[kMaxBasis / 2];
-  __shared__ double red[2][kEigThreads / 32];
-  __shared__ int s_go;
+  __shared__ int s_rot;
   for (int w = tid; w < np * np; w += nt) {
     const int i = w / np, j = w % np;
     V[i][j] = (i == j) ? 1.0 : 0.0;
     if (i >= n || j >= n) A[i][j] = 0.0;
   }
+  if (tid == 0) s_rot = 0;
   __syncthreads();
-  for (int sweep = 0; sweep < 30; ++sweep) {
-    double off = 0.0, tot = 0.0;
-    for (int w = tid; w < n * n; w += nt) {
-      const int i = w / n, j = w % n;
-      const double a = A[i][j];
-      tot += a * a;
-      if (i != j) off += a * a;
-    }
-    off = warp_sum(off);
-    tot = warp_sum(tot);
-    if ((tid & 31) == 0) { red[0][tid >> 5] = off; red[1][tid >> 5] = tot; }
-    __syncthreads();
-    if (tid == 0) {
-      double o = 0.0, t = 0.0;
-      for (int w = 0; w < (nt + 31) / 32; ++w) { o += red[0][w]; t += red[1][w]; }
-      s_go = (o > 1e-26 * t) && np >= 2;
-    }
-    __syncthreads();
-    if (!s_go) break;
+  for (int sweep = 0; sweep < kJacobiSweeps && np >= 2; ++sweep) {
     for (int r = 0; r < np - 1; ++r) {
       if (tid < np / 2) {
         const int k = tid;
@@ -115,12 +108,13 @@ __device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
         if (p > q) { const int t = p; p = q; q = t; }
         double c = 1.0, s = 0.0;
         if (q < n) {
-          const double apq = A[p][q];
-          if (apq != 0.0) {
-            const double tau = (A[q][q] - A[p][p]) / (2.0 * apq);
+          const double apq = A[p][q], app = A[p][p], aqq = A[q][q];
+          if (fabs(apq) > kJacobiRel * sqrt(fabs(app * aqq))) {
+            const double tau = (aqq - app) / (2.0 * apq);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
             s = t * c;
+            s_rot = 1;
           }
         }
         P_s[k] = p; Q_s[k] = q; cs_s[k] = c; sn_s[k] = s;
@@ -129,6 +123,7 @@ __device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
       const int npair = np / 2;
       for (int w = tid; w < npair * np; w += nt) {       // rows: A <- J^T A
         const int k = w / np, j = w % np;
+        if (sn_s[k] == 0.0) continue;
         const int p = P_s[k], q = Q_s[k];
         const double c = cs_s[k], s = sn_s[k];
         const double ap = A[p][j], aq = A[q][j];
@@ -138,6 +133,7 @@ __device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
       __syncthreads();
       for (int w = tid; w < npair * np; w += nt) {       // columns: A <- A J ; V <- V J
         const int k = w / np, j = w % np;
+        if (sn_s[k] == 0.0) continue;
         const int p = P_s[k], q = Q_s[k];
         const double c = cs_s[k], s = sn_s[k];
         const double ap = A[j][p], aq = A[j][q];
@@ -149,6 +145,11 @@ __device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
       }
       __syncthreads();
     }
+    const int rotated = s_rot;
+    __syncthreads();
+    if (tid == 0) s_rot = 0;
+    __syncthreads();
+    if (!rotated) break;
   }
 }
 
@@ -353,8 +354,25 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   cudaStreamSynchronize(s);
   if (hinfo < 0) { c.last_error = "LOBPCG: initial block is rank deficient"; return -3; }
   bool conv = false;
-  for (it = 0; it < maxiter; ++it) {
-    T* X = (T*)B.S[cur];
+  // K X, M X, K P, M P follow the update recurrence (S C) between refreshes.
+  // The recurrence mixes in K W, whose norm is up to lambda_max / lambda_1
+  // times that of K X, so its rounding error grows relative to the small
+  // wanted residuals; recomputing the products every kLobRefresh iterations
+  // (and before convergence is accepted) bounds that drift.
+  auto refresh = [&](bool with_p) -> int {
+    void* S = B.S[cur];
+    if (launch_matvec(c, 0, f64, S, B.KS[cur], nb, nullptr, s)) return -2;
+    if (launch_matvec(c, 1, f64, S, B.MS[cur], nb, nullptr, s)) return -2;
+    if (with_p) {
+      const T* P = vec<T>(S, 2 * nb, vs);
+      if (launch_matvec(c, 0, f64, P, vec<T>(B.KS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
+      if (launch_matvec(c, 1, f64, P, vec<T>(B.MS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
+    }
+    return 0;
+  };
+  double worst = 0.0;
+  bool finite = true;
+  auto residual = [&]() -> int {
     T* W = vec<T>(B.S[cur], nb, vs);
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
@@ -364,17 +382,27 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
-    double worst = 0.0;
-    bool finite = true;
+    worst = 0.0;
+    finite = true;
     for (int j = 0; j < nmodes; ++j) {
       const double r = sqrt(hr[2 * j]) / fmax(sqrt(hr[2 * j + 1]), 1e-300);
       if (!isfinite(r)) finite = false;
       worst = fmax(worst, r);
       if (resid_out) resid_out[j] = r;
     }
+    return 0;
+  };
+  for (it = 0; it < maxiter; ++it) {
+    bool fresh = it > 0 && it % kLobRefresh == 0;
+    if (fresh && refresh(true)) return -2;
+    if (residual()) return -2;
+    if (finite && worst <= tol && !fresh && it > 0) {      // confirm on fresh products
+      if (refresh(true) || residual()) return -2;
+    }
     if (hinfo < 0) { c.last_error = "LOBPCG: Rayleigh-Ritz basis rank deficient"; return -3; }
     if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
     if (worst <= tol) { conv = true; break; }
+    T* W = vec<T>(B.S[cur], nb, vs);
     if (precond == 2) {
       // W <- V-cycle(W): the FP32 multigrid approximation of K^-1
       if (mg_ensure(c, s)) return -2;
@@ -406,7 +434,6 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     launch_lob_update<T>(NN, nb, ncols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
                          (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
     cur ^= 1;
-    (void)X;
   }
   if (iters_out) *iters_out = it;
   // final FP64 Rayleigh-Ritz on fresh FP64 products
