@@ -102,6 +102,14 @@ int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float
 void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s);
 void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s);
 void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s);
+// Column selection of a node4 block: vector k of the selection is vector
+// col[k] of the block (up to 24).
+struct ColMap {
+  int col[24];
+};
+// G = A[:, ma]^T B[:, mb] (na x nb), same kernels as launch_gram
+void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na, const void* B, const ColMap& mb,
+                      int nb, double* G, cudaStream_t s);
 void launch_quadform(const Ctx& c, int op, bool f64, const void* v, int nvec, double* out, cudaStream_t s);
 void launch_convert(const void* src, bool src64, void* dst, bool dst64, long long n, cudaStream_t s);
 void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s);

@@ -298,9 +298,9 @@ constexpr int kGramChunk = 24;                       // nodes per staged chunk
 constexpr int kGramLd = 4 * kGramChunk + 2;          // doubles per staged vector row
 
 template <typename T>
-__global__ void __launch_bounds__(kGramThreads) k_gram_partial(int NN, const T* __restrict__ A, int na,
-                                                              const T* __restrict__ B, int nb, long long vstride,
-                                                              double* part) {
+__global__ void __launch_bounds__(kGramThreads) k_gram_partial(int NN, const T* __restrict__ A, ColMap ma, int na,
+                                                              const T* __restrict__ B, ColMap mb, int nb,
+                                                              long long vstride, double* part) {
   using V4 = typename Vec4<T>::type;
   __shared__ __align__(16) double sm[48 * kGramLd];   // rows 0..23: A, 24..47: B
   static_assert(48 * kGramLd >= 8 * 576, "reduction scratch");
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kGramThreads) k_gram_partial(int NN, const T* 
       const int v = idx / kGramChunk, q = idx % kGramChunk;
       if (q >= cnt) continue;
       const bool isA = v < na;
-      const T* src = isA ? A + v * vstride : B + (v - na) * vstride;
+      const T* src = isA ? A + ma.col[v] * vstride : B + mb.col[v - na] * vstride;
       const V4 x = reinterpret_cast<const V4*>(src)[n0 + q];
       double* d = (isA ? sA + v * kGramLd : sB + (v - na) * kGramLd) + 4 * q;
       reinterpret_cast<double2*>(d)[0] = make_double2(double(x.x), double(x.y));
@@ -377,20 +377,27 @@ __global__ void __launch_bounds__(256) k_gram_reduce(int nblocks, int npair, con
   if (lane == 0) G[p] = s;
 }
 
-void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s) {
+void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na, const void* B, const ColMap& mb,
+                      int nb, double* G, cudaStream_t s) {
   const int nchunks = ceil_div(c.g.NN, kGramChunk);
   int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
   if (blocks < 1) blocks = 1;
   const long long vs = (long long)c.g.NN * 4;
   if (f64)
-    k_gram_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, na, (const double*)B, nb, vs,
-                                                          c.gram_part);
+    k_gram_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, ma, na, (const double*)B, mb,
+                                                          nb, vs, c.gram_part);
   else
-    k_gram_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, na, (const float*)B, nb, vs,
-                                                         c.gram_part);
+    k_gram_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, ma, na, (const float*)B, mb, nb,
+                                                         vs, c.gram_part);
   count_launch();
   k_gram_reduce<<<ceil_div(na * nb, 8), 256, 0, s>>>(blocks, na * nb, c.gram_part, G);
   count_launch();
+}
+
+void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s) {
+  ColMap id;
+  for (int k = 0; k < 24; ++k) id.col[k] = k;
+  launch_gram_cols(c, f64, A, id, na, B, id, nb, G, s);
 }
 
 // ---------------------------------------------------------------------------

@@ -17,6 +17,7 @@
 // freshly computed FP64 K X, M X gives the eigenvalues; in FP64 mode
 // everything is FP64.
 #include <math.h>
+#include <stdio.h>
 
 #include "tof_internal.h"
 #include "tof_stencil.cuh"
@@ -30,13 +31,15 @@ constexpr int kMaxBasis = 24;
 constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M products
 
 // ---------------------------------------------------------------------------
-// residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, and per-CTA
-// partial sums of ||W_j||^2 and ||KX_j||^2 (unscaled residual)
+// residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, written to
+// vector wslot.col[j] of S (skipped for wslot.col[j] < 0: a soft-locked
+// column), and the norms ||W_j||^2, ||KX_j||^2 (unscaled residual) of every
+// column, reduced by the last CTA into out[2j], out[2j+1]
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs, const T* __restrict__ KX,
                                                    const T* __restrict__ MX, const double* __restrict__ theta,
-                                                   const T* __restrict__ dinv, T* W, double* part,
+                                                   const T* __restrict__ dinv, T* S, ColMap wslot, double* part,
                                                    unsigned* counter, double* out) {
   using V4 = typename Vec4<T>::type;
   __shared__ double red[16 * 32];
@@ -58,7 +61,7 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
       v[2 * j] += double(w.x) * w.x + double(w.y) * w.y + double(w.z) * w.z;
       v[2 * j + 1] += double(kx.x) * kx.x + double(kx.y) * kx.y + double(kx.z) * kx.z;
       if (dinv) { w.x *= di.x; w.y *= di.y; w.z *= di.z; }
-      reinterpret_cast<V4*>(W)[o] = w;
+      if (wslot.col[j] >= 0) reinterpret_cast<V4*>(S + wslot.col[j] * vs)[n] = w;
     }
   }
   double tot[16];
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
 // outputs, all in registers.  The 4th (padding) component of the outputs is
 // never written and stays zero.
 template <typename T>
-__global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, long long vs,
+__global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, ColMap cols, long long vs,
                                                     const T* __restrict__ S, const T* __restrict__ KS,
                                                     const T* __restrict__ MS, const double* __restrict__ C,
                                                     T* S2, T* KS2, T* MS2) {
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, l
   const size_t o = 4 * (size_t)n + c;
   T in[kMaxBasis];
 #pragma unroll
-  for (int j = 0; j < kMaxBasis; ++j) in[j] = j < ncols ? src[j * vs + o] : T(0);
+  for (int j = 0; j < kMaxBasis; ++j) in[j] = j < ncols ? src[cols.col[j] * vs + o] : T(0);
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     if (k >= nb) break;
@@ -274,11 +277,19 @@ __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, l
   }
 }
 
+// X' = S[:, cols] C (first nb vectors of the destination), P' = the part of
+// that product from the columns after the first nb (vectors 2 nb .. 3 nb - 1)
 template <typename T>
-static void launch_lob_update(int NN, int nb, int ncols, long long vs, const T* S, const T* KS, const T* MS,
-                              const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s) {
-  k_lob_update<T><<<int((9LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, vs, S, KS, MS, C, S2, KS2, MS2);
+static void launch_lob_update(int NN, int nb, int ncols, const ColMap& cols, long long vs, const T* S, const T* KS,
+                              const T* MS, const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s) {
+  k_lob_update<T><<<int((9LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2);
   count_launch();
+}
+
+static ColMap identity_cols() {
+  ColMap m;
+  for (int k = 0; k < 24; ++k) m.col[k] = k;
+  return m;
 }
 
 // ---------------------------------------------------------------------------
@@ -343,7 +354,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   launch_gram(c, f64, B.S[cur], nb, B.KS[cur], nb, GK, s);
   launch_gram(c, f64, B.S[cur], nb, B.MS[cur], nb, GM, s);
   lob_small_eig(c, nb, nb, drop, s);
-  launch_lob_update<T>(NN, nb, nb, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
+  const ColMap ident = identity_cols();
+  launch_lob_update<T>(NN, nb, nb, ident, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
                        (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
   cur ^= 1;
   int it = 0;
@@ -359,25 +371,38 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   // times that of K X, so its rounding error grows relative to the small
   // wanted residuals; recomputing the products every kLobRefresh iterations
   // (and before convergence is accepted) bounds that drift.
-  auto refresh = [&](bool with_p) -> int {
+  auto refresh = [&]() -> int {
     void* S = B.S[cur];
     if (launch_matvec(c, 0, f64, S, B.KS[cur], nb, nullptr, s)) return -2;
     if (launch_matvec(c, 1, f64, S, B.MS[cur], nb, nullptr, s)) return -2;
-    if (with_p) {
-      const T* P = vec<T>(S, 2 * nb, vs);
-      if (launch_matvec(c, 0, f64, P, vec<T>(B.KS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
-      if (launch_matvec(c, 1, f64, P, vec<T>(B.MS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
-    }
+    const T* P = vec<T>(S, 2 * nb, vs);
+    if (launch_matvec(c, 0, f64, P, vec<T>(B.KS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
+    if (launch_matvec(c, 1, f64, P, vec<T>(B.MS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
     return 0;
+  };
+  // Soft locking (as scipy.sparse.linalg.lobpcg's active mask): a wanted
+  // column whose residual is below tol leaves the search space [W, P] but
+  // stays in X, so later Rayleigh-Ritz steps still refine it.  Tiny residual
+  // columns otherwise make the basis ill-conditioned and stall the slowest
+  // (lowest) modes.  Guard columns (j >= nmodes) are never locked.
+  bool locked[8] = {false, false, false, false, false, false, false, false};
+  double rres[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int act[8];
+  ColMap wslot;
+  auto active_map = [&]() -> int {   // W_j of active column j goes to vector nb + k
+    int k = 0;
+    for (int j = 0; j < 24; ++j) wslot.col[j] = -1;
+    for (int j = 0; j < nb; ++j)
+      if (!locked[j]) { act[k] = j; wslot.col[j] = nb + k; ++k; }
+    return k;
   };
   double worst = 0.0;
   bool finite = true;
   auto residual = [&]() -> int {
-    T* W = vec<T>(B.S[cur], nb, vs);
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
-    k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, W, c.gram_part,
-                                           c.counters, rn);
+    k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, (T*)B.S[cur],
+                                           wslot, c.gram_part, c.counters, rn);
     count_launch();
     cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
@@ -388,51 +413,80 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       const double r = sqrt(hr[2 * j]) / fmax(sqrt(hr[2 * j + 1]), 1e-300);
       if (!isfinite(r)) finite = false;
       worst = fmax(worst, r);
+      rres[j] = r;
       if (resid_out) resid_out[j] = r;
     }
     return 0;
   };
   for (it = 0; it < maxiter; ++it) {
-    bool fresh = it > 0 && it % kLobRefresh == 0;
-    if (fresh && refresh(true)) return -2;
+    const bool fresh = it > 0 && it % kLobRefresh == 0;
+    if (fresh && refresh()) return -2;
+    int na = active_map();
     if (residual()) return -2;
-    if (finite && worst <= tol && !fresh && it > 0) {      // confirm on fresh products
-      if (refresh(true) || residual()) return -2;
+    if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
+    bool changed = false, all = true;
+    for (int j = 0; j < nmodes; ++j) {
+      if (!locked[j] && rres[j] <= tol) { locked[j] = true; changed = true; }
+      all = all && locked[j];
     }
+    if (all) {                                 // confirm on fresh products
+      if (!fresh && it > 0 && refresh()) return -2;
+      active_map();
+      if (residual()) return -2;
+      bool reopened = false;
+      for (int j = 0; j < nmodes; ++j)
+        if (!(rres[j] <= tol)) { locked[j] = false; reopened = true; }
+      if (!reopened) { conv = true; break; }
+      changed = true;
+    }
+    if (changed) {                             // W of the new active set
+      na = active_map();
+      if (residual()) return -2;
+    }
+#ifdef TOF_LOB_TRACE
+    fprintf(stderr, "lobpcg it %d rank %d active %d fresh %d worst %.3e res", it, hinfo, na, int(fresh), worst);
+    for (int j = 0; j < nmodes; ++j) fprintf(stderr, " %.2e", rres[j]);
+    fprintf(stderr, " theta0 %.10e\n", hth[0]);
+#endif
     if (hinfo < 0) { c.last_error = "LOBPCG: Rayleigh-Ritz basis rank deficient"; return -3; }
     if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
-    if (worst <= tol) { conv = true; break; }
     T* W = vec<T>(B.S[cur], nb, vs);
+    const int R = na <= 1 ? 1 : na <= 2 ? 2 : na <= 4 ? 4 : 8;
     if (precond == 2) {
       // W <- V-cycle(W): the FP32 multigrid approximation of K^-1
       if (mg_ensure(c, s)) return -2;
-      const int R = nb <= 1 ? 1 : nb <= 2 ? 2 : nb <= 4 ? 4 : 8;
       float* r32 = mg_rhs(c);
-      if (R > nb) cudaMemsetAsync(r32, 0, sizeof(float) * R * vs, s);
-      launch_convert(W, f64, r32, false, (long long)nb * vs, s);
+      if (R > na) cudaMemsetAsync(r32, 0, sizeof(float) * R * vs, s);
+      launch_convert(W, f64, r32, false, (long long)na * vs, s);
       if (mg_vcycle(c, R, s)) return -2;
-      launch_convert(mg_out(c), false, W, f64, (long long)nb * vs, s);
+      launch_convert(mg_out(c), false, W, f64, (long long)na * vs, s);
     } else if (precond == 1) {
-      // W <- (inexact) K^-1 W by the pipelined block PCG (FP32)
+      // W <- (inexact) K^-1 W by block PCG (FP32)
       const size_t pblk = (size_t)c.max_rhs * vs;
       double* b64 = c.pw64 + 6 * pblk;
       float* d32 = c.pw32 + 9 * pblk;
-      int R = nb <= 1 ? 1 : nb <= 2 ? 2 : nb <= 4 ? 4 : 8;
       cudaMemsetAsync(b64, 0, sizeof(double) * R * vs, s);
-      launch_convert(W, f64, b64, true, (long long)nb * vs, s);
+      launch_convert(W, f64, b64, true, (long long)na * vs, s);
       cudaMemsetAsync(d32, 0, sizeof(float) * R * vs, s);
       if (pcg_std32(c, b64, d32, R, inner_rtol, inner_iters, s)) return -2;
-      launch_convert(d32, false, W, f64, (long long)nb * vs, s);
+      launch_convert(d32, false, W, f64, (long long)na * vs, s);
     }
-    const int ncols = it == 0 ? 2 * nb : 3 * nb;
-    if (launch_matvec(c, 0, f64, W, vec<T>(B.KS[cur], nb, vs), nb, nullptr, s)) return -2;
-    if (launch_matvec(c, 1, f64, W, vec<T>(B.MS[cur], nb, vs), nb, nullptr, s)) return -2;
-    launch_gram(c, f64, B.S[cur], ncols, B.KS[cur], ncols, GK, s);
-    launch_gram(c, f64, B.S[cur], ncols, B.MS[cur], ncols, GM, s);
+    if (launch_matvec(c, 0, f64, W, vec<T>(B.KS[cur], nb, vs), na, nullptr, s)) return -2;
+    if (launch_matvec(c, 1, f64, W, vec<T>(B.MS[cur], nb, vs), na, nullptr, s)) return -2;
+    // basis [X, W_active, P_active]
+    ColMap cols;
+    int ncols = 0;
+    for (int j = 0; j < nb; ++j) cols.col[ncols++] = j;
+    for (int k = 0; k < na; ++k) cols.col[ncols++] = nb + k;
+    if (it > 0)
+      for (int k = 0; k < na; ++k) cols.col[ncols++] = 2 * nb + act[k];
+    for (int k = ncols; k < 24; ++k) cols.col[k] = 0;
+    launch_gram_cols(c, f64, B.S[cur], cols, ncols, B.KS[cur], cols, ncols, GK, s);
+    launch_gram_cols(c, f64, B.S[cur], cols, ncols, B.MS[cur], cols, ncols, GM, s);
     lob_small_eig(c, ncols, nb, drop, s);
     cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
-    launch_lob_update<T>(NN, nb, ncols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
-                         (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
+    launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
+                         (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
     cur ^= 1;
   }
   if (iters_out) *iters_out = it;
@@ -453,7 +507,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     // reuse the update kernel: S = X6 (ncols = nb), P part unused -> KS2/MS2 scratch
     double* scratch = c.lw64 + 3LL * c.max_modes * vs;   // FP64 LOBPCG area (free in mixed mode)
     if (f64) scratch = (double*)B.S[cur ^ 1];
-    launch_lob_update<double>(NN, nb, nb, vs, X6, KX6, MX6, C, scratch, scratch + 3LL * c.max_modes * vs,
+    launch_lob_update<double>(NN, nb, nb, ident, vs, X6, KX6, MX6, C, scratch, scratch + 3LL * c.max_modes * vs,
                               scratch + 6LL * c.max_modes * vs, s);
     cudaMemcpyAsync(out, scratch, sizeof(double) * nmodes * vs, cudaMemcpyDeviceToDevice, s);
   }
