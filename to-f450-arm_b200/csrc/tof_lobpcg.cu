@@ -72,165 +72,290 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
 }
 
 // ---------------------------------------------------------------------------
-// CTA-parallel cyclic Jacobi eigensolver for a symmetric positive
-// semi-definite n x n (n <= 24) matrix held in shared memory.  Round-robin
-// ordering applies n/2 disjoint rotations per step (rows, then columns and
-// the eigenvector matrix), each element update by its own thread.  A pair
-// (p, q) is rotated only while |a_pq| > kJacobiRel * sqrt(a_pp a_qq); the
-// iteration stops after a sweep without rotations.  That relative test
-// (Demmel & Veselic, SIAM J. Matrix Anal. Appl. 13 (1992)) keeps the small
-// eigenvalues and their eigenvectors accurate to working precision relative
-// to themselves, which the Rayleigh-Ritz step needs: its projected matrices
-// span the whole spectrum of K, and the wanted pairs sit at the bottom.
-// Rotation: Golub & Van Loan, Matrix Computations, Alg. 8.4.1 (sym.schur2).
+// Symmetric eigensolver for n <= 24, one warp, matrix in shared memory:
+// Householder tridiagonalisation (Golub & Van Loan, Matrix Computations,
+// 4th ed., Alg. 8.3.1) with the reflections accumulated into Q, then the
+// implicit symmetric QR step with Wilkinson shift (Alg. 8.3.2) inside the
+// deflation loop of Alg. 8.3.3.  Lane i owns row i of A and Q.  The warp
+// tests the off-diagonals for deflation in parallel (ballot); lane 0 chases
+// the bulge on the (d, e) diagonals with rsqrt-based Givens rotations and
+// records them; the warp then applies the recorded rotations to the rows of
+// Q.  Backward stable: eigenvalue errors ~ eps ||A||.
+// On return d[k] / Q[:, k] are the eigenpairs (unsorted); false if the QR
+// iteration did not converge within its sweep budget.
 // ---------------------------------------------------------------------------
 constexpr int LDA = kMaxBasis + 1;
-constexpr int kEigThreads = 128;
-constexpr double kJacobiRel = 1e-15;
-constexpr int kJacobiSweeps = 40;
+constexpr int kEigThreads = 32;
+constexpr int kQrSweeps = 30 * kMaxBasis;
 
-__device__ void cta_jacobi(double (*A)[LDA], double (*V)[LDA], int n) {
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int np = n + (n & 1);
-  __shared__ double cs_s[kMaxBasis / 2], sn_s[kMaxBasis / 2];
-  __shared__ int P_s[kMaxBasis / 2], Q_s[kMaxBasis / 2];
-  __shared__ int s_rot;
-  for (int w = tid; w < np * np; w += nt) {
-    const int i = w / np, j = w % np;
-    V[i][j] = (i == j) ? 1.0 : 0.0;
-    if (i >= n || j >= n) A[i][j] = 0.0;
-  }
-  if (tid == 0) s_rot = 0;
-  __syncthreads();
-  for (int sweep = 0; sweep < kJacobiSweeps && np >= 2; ++sweep) {
-    for (int r = 0; r < np - 1; ++r) {
-      if (tid < np / 2) {
-        const int k = tid;
-        auto pos = [&](int q) { return q == 0 ? 0 : 1 + ((q - 1 + r) % (np - 1)); };
-        int p = pos(k), q = pos(np - 1 - k);
-        if (p > q) { const int t = p; p = q; q = t; }
-        double c = 1.0, s = 0.0;
-        if (q < n) {
-          const double apq = A[p][q], app = A[p][p], aqq = A[q][q];
-          if (fabs(apq) > kJacobiRel * sqrt(fabs(app * aqq))) {
-            const double tau = (aqq - app) / (2.0 * apq);
-            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            c = 1.0 / sqrt(1.0 + t * t);
-            s = t * c;
-            s_rot = 1;
-          }
-        }
-        P_s[k] = p; Q_s[k] = q; cs_s[k] = c; sn_s[k] = s;
-      }
-      __syncthreads();
-      const int npair = np / 2;
-      for (int w = tid; w < npair * np; w += nt) {       // rows: A <- J^T A
-        const int k = w / np, j = w % np;
-        if (sn_s[k] == 0.0) continue;
-        const int p = P_s[k], q = Q_s[k];
-        const double c = cs_s[k], s = sn_s[k];
-        const double ap = A[p][j], aq = A[q][j];
-        A[p][j] = c * ap - s * aq;
-        A[q][j] = s * ap + c * aq;
-      }
-      __syncthreads();
-      for (int w = tid; w < npair * np; w += nt) {       // columns: A <- A J ; V <- V J
-        const int k = w / np, j = w % np;
-        if (sn_s[k] == 0.0) continue;
-        const int p = P_s[k], q = Q_s[k];
-        const double c = cs_s[k], s = sn_s[k];
-        const double ap = A[j][p], aq = A[j][q];
-        A[j][p] = c * ap - s * aq;
-        A[j][q] = s * ap + c * aq;
-        const double vp = V[j][p], vq = V[j][q];
-        V[j][p] = c * vp - s * vq;
-        V[j][q] = s * vp + c * vq;
-      }
-      __syncthreads();
+struct EigScratch {
+  double e[kMaxBasis], rc[kMaxBasis], rs[kMaxBasis], v[kMaxBasis], w[kMaxBasis];
+};
+
+__device__ bool warp_syev(double (*A)[LDA], double (*Q)[LDA], double* d, EigScratch& S, int n) {
+  const int lane = threadIdx.x;
+  const unsigned full = 0xffffffffu;
+  double* e = S.e;
+  double* v = S.v;
+  double* w = S.w;
+  for (int j = 0; j < n; ++j)
+    if (lane < n) Q[lane][j] = (lane == j) ? 1.0 : 0.0;
+  __syncwarp();
+  // --- tridiagonalisation: A <- H_k A H_k, Q <- Q H_k
+  for (int k = 0; k + 2 < n; ++k) {
+    const int i = lane;
+    const bool below = i > k && i < n;
+    const double xi = below ? A[i][k] : 0.0;
+    const double sig = warp_sum((i > k + 1 && i < n) ? xi * xi : 0.0);
+    const double alpha = __shfl_sync(full, xi, k + 1);
+    if (!(sig > 0.0)) {                    // column already reduced
+      __syncwarp();
+      continue;
     }
-    const int rotated = s_rot;
-    __syncthreads();
-    if (tid == 0) s_rot = 0;
-    __syncthreads();
-    if (!rotated) break;
+    const double mu = sqrt(alpha * alpha + sig);
+    const double v1 = alpha <= 0.0 ? alpha - mu : -sig / (alpha + mu);
+    const double beta = 2.0 * v1 * v1 / (sig + v1 * v1);
+    if (below) v[i] = (i == k + 1) ? 1.0 : xi / v1;
+    __syncwarp();
+    // p = beta A' v, w = p - (beta / 2)(p^T v) v
+    double p = 0.0;
+    if (below)
+      for (int j = k + 1; j < n; ++j) p = fma(A[i][j], v[j], p);
+    p *= beta;
+    const double pv = warp_sum(below ? p * v[i] : 0.0);
+    if (below) w[i] = p - 0.5 * beta * pv * v[i];
+    double sq = 0.0;                       // (Q v)_i
+    if (i < n)
+      for (int j = k + 1; j < n; ++j) sq = fma(Q[i][j], v[j], sq);
+    __syncwarp();
+    if (below)
+      for (int j = k + 1; j < n; ++j) A[i][j] -= v[i] * w[j] + w[i] * v[j];
+    if (i < n)
+      for (int j = k + 1; j < n; ++j) Q[i][j] -= beta * sq * v[j];
+    if (i == k + 1) { A[k + 1][k] = mu; A[k][k + 1] = mu; }
+    if (i > k + 1 && i < n) { A[i][k] = 0.0; A[k][i] = 0.0; }
+    __syncwarp();
   }
+  if (lane < n) d[lane] = A[lane][lane];
+  if (lane + 1 < n) e[lane] = A[lane + 1][lane];
+  __syncwarp();
+  // --- implicit symmetric QR on (d, e)
+  const double eps = 2.220446049250313e-16;
+  for (int sweep = 0; sweep < kQrSweeps; ++sweep) {
+    bool live = false;
+    if (lane + 1 < n) {
+      if (fabs(e[lane]) <= eps * (fabs(d[lane]) + fabs(d[lane + 1]))) e[lane] = 0.0;
+      else live = true;
+    }
+    const unsigned bits = __ballot_sync(full, live);
+    __syncwarp();
+    if (bits == 0u) return true;
+    const int top = 31 - __clz(bits);      // last nonzero off-diagonal
+    const int hi = top + 1;
+    const unsigned zeros = ~bits & ((1u << top) - 1u);
+    const int lo = zeros ? 32 - __clz(zeros) : 0;
+    if (lane == 0) {
+      // Wilkinson shift from the trailing 2 x 2 of the block
+      const double dl = 0.5 * (d[hi - 1] - d[hi]);
+      const double eh = e[hi - 1];
+      const double sg = dl >= 0.0 ? 1.0 : -1.0;
+      const double mu = d[hi] - eh * eh / (dl + sg * sqrt(dl * dl + eh * eh));
+      double x = d[lo] - mu, z = e[lo], bulge = 0.0;
+      double dk = d[lo], ek = e[lo];
+      for (int k = lo; k < hi; ++k) {
+        if (k > lo) { x = e[k - 1]; z = bulge; }
+        const double r2 = x * x + z * z;
+        double c = 1.0, sn = 0.0, r = 0.0;
+        if (r2 > 0.0) {
+          const double ir = rsqrt(r2);
+          c = x * ir; sn = z * ir; r = r2 * ir;
+        }
+        if (k > lo) e[k - 1] = r;
+        const double dd = d[k + 1];
+        const double a = dk, b = ek;
+        const double cc = c * c, ss = sn * sn, cs = c * sn;
+        d[k] = cc * a + 2.0 * cs * b + ss * dd;
+        dk = ss * a - 2.0 * cs * b + cc * dd;   // new d[k + 1]
+        e[k] = cs * (dd - a) + (cc - ss) * b;
+        d[k + 1] = dk;
+        if (k + 1 < hi) {
+          const double en = e[k + 1];
+          bulge = sn * en;
+          ek = c * en;
+          e[k + 1] = ek;
+        }
+        S.rc[k] = c; S.rs[k] = sn;
+      }
+    }
+    __syncwarp();
+    if (lane < n) {
+      for (int k = lo; k < hi; ++k) {       // Q <- Q G_k
+        const double c = S.rc[k], sn = S.rs[k];
+        const double qa = Q[lane][k], qb = Q[lane][k + 1];
+        Q[lane][k] = c * qa + sn * qb;
+        Q[lane][k + 1] = -sn * qa + c * qb;
+      }
+    }
+    __syncwarp();
+  }
+  return false;
+}
+
+// In-place Cholesky B = L L^T of a symmetric n x n matrix (lower triangle
+// and diagonal become L); idiag[k] = 1 / L[k][k].  false (uniformly across
+// the warp) when a pivot is not above piv_min: the basis is too close to
+// dependent for Cholesky-based orthonormalisation.
+__device__ bool warp_chol(double (*B)[LDA], double* idiag, int n, double piv_min) {
+  const int lane = threadIdx.x;
+  for (int k = 0; k < n; ++k) {
+    const double pk = B[k][k];
+    if (!(pk > piv_min)) return false;
+    const double ir = rsqrt(pk);
+    __syncwarp();
+    if (lane > k && lane < n) B[lane][k] *= ir;
+    if (lane == k) { B[k][k] = pk * ir; idiag[k] = ir; }
+    __syncwarp();
+    if (lane > k && lane < n) {
+      const double lik = B[lane][k];
+      for (int j = k + 1; j <= lane; ++j) B[lane][j] -= lik * B[j][k];
+    }
+    __syncwarp();
+  }
+  return true;
 }
 
 // Rayleigh-Ritz: the m smallest eigenpairs of G_K c = theta G_M c (n x n).
-// G_M is scaled to unit diagonal and eigendecomposed; directions with
-// eigenvalue below drop_tol * max are discarded (a near-dependent basis), and
-// the standard problem is solved in the remaining orthonormal basis.
+// Both Grams are scaled by D = diag(G_M)^-1/2.  Fast path: Cholesky
+// D G_M D = L L^T (pivots above kCholPivot, i.e. a well-conditioned basis)
+// and the standard problem L^-1 (D G_K D) L^-T.  Otherwise the SVQB form
+// (Stathopoulos & Wu, SIAM J. Sci. Comput. 23 (2002)): D G_M D is
+// eigendecomposed, directions with eigenvalue below drop_tol * max are
+// discarded, and the standard problem is solved in the remaining
+// M-orthonormal basis.
 // Outputs: C (n x m, row-major), theta (m), info[0] = kept rank (or -1).
+constexpr double kCholPivot = 1e-8;
+
 __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const double* __restrict__ GK,
                                                           const double* __restrict__ GM, double drop_tol, double* C,
                                                           double* theta, int* info) {
   __shared__ double A[kMaxBasis][LDA], B[kMaxBasis][LDA], V[kMaxBasis][LDA], Z[kMaxBasis][LDA];
-  __shared__ double D[kMaxBasis], ev[kMaxBasis];
+  __shared__ double D[kMaxBasis], ev[kMaxBasis], idg[kMaxBasis];
+  __shared__ EigScratch S;
   __shared__ int keep[kMaxBasis], order[kMaxBasis];
   __shared__ int kr;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int w = tid; w < n; w += nt) {
-    const double b = GM[w * n + w];
-    D[w] = b > 0.0 ? 1.0 / sqrt(b) : 0.0;
+  const int lane = threadIdx.x;
+  if (lane < n) {
+    const double b = GM[lane * n + lane];
+    D[lane] = b > 0.0 ? 1.0 / sqrt(b) : 0.0;
   }
-  __syncthreads();
-  for (int w = tid; w < n * n; w += nt) {
+  __syncwarp();
+  for (int w = lane; w < n * n; w += 32) {
     const int i = w / n, j = w % n;
     A[i][j] = 0.5 * (GK[i * n + j] + GK[j * n + i]) * D[i] * D[j];
     B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
   }
-  __syncthreads();
-  cta_jacobi(B, V, n);
-  if (tid == 0) {
-    double bmax = 0.0;
-    for (int i = 0; i < n; ++i) bmax = fmax(bmax, B[i][i]);
-    int k = 0;
-    for (int i = 0; i < n; ++i)
-      if (D[i] > 0.0 && B[i][i] > drop_tol * bmax) keep[k++] = i;
-    kr = k;
+  __syncwarp();
+  bool ok = true;
+  int K = n;
+  const bool chol = warp_chol(B, idg, n, kCholPivot);
+  if (chol) {
+    // V = L^-1 A (lane j: column j), then Z = V L^-T (lane j: row j of Z)
+    if (lane < n) {
+      for (int i = 0; i < n; ++i) {
+        double t = A[i][lane];
+        for (int l = 0; l < i; ++l) t = fma(-B[i][l], V[l][lane], t);
+        V[i][lane] = t * idg[i];
+      }
+    }
+    __syncwarp();
+    if (lane < n) {
+      for (int i = 0; i < n; ++i) {
+        double t = V[lane][i];
+        for (int l = 0; l < i; ++l) t = fma(-B[i][l], Z[lane][l], t);
+        Z[lane][i] = t * idg[i];
+      }
+    }
+    __syncwarp();
+    for (int w = lane; w < n * n; w += 32) {
+      const int a = w / n, b = w % n;
+      A[a][b] = 0.5 * (Z[a][b] + Z[b][a]);
+    }
+    __syncwarp();
+  } else {
+    for (int w = lane; w < n * n; w += 32) {             // B was overwritten by the failed Cholesky
+      const int i = w / n, j = w % n;
+      B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
+    }
+    __syncwarp();
+    ok = warp_syev(B, V, ev, S, n);
+    if (lane == 0) {
+      double bmax = 0.0;
+      for (int i = 0; i < n; ++i) bmax = fmax(bmax, ev[i]);
+      int k = 0;
+      for (int i = 0; i < n; ++i)
+        if (ev[i] > drop_tol * bmax) keep[k++] = i;
+      kr = k;
+    }
+    __syncwarp();
+    K = kr;
+    for (int w = lane; w < n * K; w += 32) {              // Z = V[:, keep] / sqrt(lambda)
+      const int i = w / K, a = w % K;
+      Z[i][a] = V[i][keep[a]] / sqrt(ev[keep[a]]);
+    }
+    __syncwarp();
+    for (int w = lane; w < n * K; w += 32) {              // V <- A Z
+      const int i = w / K, a = w % K;
+      double s = 0.0;
+      for (int j = 0; j < n; ++j) s = fma(A[i][j], Z[j][a], s);
+      V[i][a] = s;
+    }
+    __syncwarp();
+    for (int w = lane; w < K * K; w += 32) {              // B <- Z^T V
+      const int a = w / K, b = w % K;
+      double s = 0.0;
+      for (int j = 0; j < n; ++j) s = fma(Z[j][a], V[j][b], s);
+      B[a][b] = s;
+    }
+    __syncwarp();
+    for (int w = lane; w < K * K; w += 32) {
+      const int a = w / K, b = w % K;
+      A[a][b] = 0.5 * (B[a][b] + B[b][a]);
+    }
+    __syncwarp();
   }
-  __syncthreads();
-  const int K = kr;
-  for (int w = tid; w < n * K; w += nt) {                 // Z = V[:, keep] / sqrt(lambda)
-    const int i = w / K, a = w % K;
-    Z[i][a] = V[i][keep[a]] / sqrt(B[keep[a]][keep[a]]);
-  }
-  __syncthreads();
-  for (int w = tid; w < n * K; w += nt) {                 // V <- A Z
-    const int i = w / K, a = w % K;
-    double s = 0.0;
-    for (int j = 0; j < n; ++j) s = fma(A[i][j], Z[j][a], s);
-    V[i][a] = s;
-  }
-  __syncthreads();
-  for (int w = tid; w < K * K; w += nt) {                 // B <- Z^T V
-    const int a = w / K, b = w % K;
-    double s = 0.0;
-    for (int j = 0; j < n; ++j) s = fma(Z[j][a], V[j][b], s);
-    B[a][b] = s;
-  }
-  __syncthreads();
-  for (int w = tid; w < K * K; w += nt) {
-    const int a = w / K, b = w % K;
-    A[a][b] = 0.5 * (B[a][b] + B[b][a]);
-  }
-  __syncthreads();
-  cta_jacobi(A, V, K);
-  if (tid == 0) {
-    for (int i = 0; i < K; ++i) { ev[i] = A[i][i]; order[i] = i; }
+  ok = warp_syev(A, V, ev, S, K) && ok;
+  if (lane == 0) {
+    for (int i = 0; i < K; ++i) order[i] = i;
     for (int i = 0; i < K; ++i)
       for (int j = i + 1; j < K; ++j)
         if (ev[order[j]] < ev[order[i]]) { const int t = order[i]; order[i] = order[j]; order[j] = t; }
-    info[0] = K >= m ? K : -1;
+    info[0] = (K >= m && ok) ? K : -1;
   }
-  __syncthreads();
-  if (K < m) return;
-  for (int w = tid; w < m; w += nt) theta[w] = ev[order[w]];
-  for (int w = tid; w < n * m; w += nt) {                 // C = D Z U[:, order[:m]]
-    const int i = w / m, k = w % m;
-    double s = 0.0;
-    for (int a = 0; a < K; ++a) s = fma(Z[i][a], V[a][order[k]], s);
-    C[i * m + k] = D[i] * s;
+  __syncwarp();
+  if (K < m || !ok) return;
+  if (lane < m) theta[lane] = ev[order[lane]];
+  if (chol) {
+    // C[:, k] = D L^-T U[:, order[k]]: lane k back-substitutes its column
+    if (lane < m) {
+      const int o = order[lane];
+      for (int i = n - 1; i >= 0; --i) {
+        double t = V[i][o];
+        for (int l = i + 1; l < n; ++l) t = fma(-B[l][i], Z[l][lane], t);
+        Z[i][lane] = t * idg[i];
+      }
+    }
+    __syncwarp();
+    for (int w = lane; w < n * m; w += 32) {
+      const int i = w / m, k = w % m;
+      C[i * m + k] = D[i] * Z[i][k];
+    }
+  } else {
+    for (int w = lane; w < n * m; w += 32) {              // C = D Z U[:, order[:m]]
+      const int i = w / m, k = w % m;
+      double s = 0.0;
+      for (int a = 0; a < K; ++a) s = fma(Z[i][a], V[a][order[k]], s);
+      C[i * m + k] = D[i] * s;
+    }
   }
 }
 
