@@ -74,6 +74,10 @@ struct MG {
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t gnodes[4] = {0, 0, 0, 0};
   bool graph_failed = false;
+  // a single V-cycle per R, replayed by callers outside the PCG graphs
+  cudaGraphExec_t vexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t vnodes[4] = {0, 0, 0, 0};
+  bool vgraph_failed = false;
 };
 constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
 
@@ -83,6 +87,74 @@ constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
 __device__ __forceinline__ void node_ijk(int n, int NX, int NY, int& i, int& j, int& k) {
   i = n % NX; j = (n / NX) % NY; k = n / (NX * NY);
 }
+
+
+// Transfer weights along one axis.  Restriction: fine offsets -1, 0, +1
+// around 2I (weights 1/2, 1, 1/2) when the axis is coarsened, else only the
+// offset 0; a fine index outside the grid gets weight 0 and a clamped index.
+__device__ __forceinline__ void restrict_axis(int f, int I, int Nf, int* idx, float* w) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int o = d - 1;
+    const int i = f * I + o;
+    const bool ok = (f == 2 || o == 0) && i >= 0 && i < Nf;
+    idx[d] = min(max(i, 0), Nf - 1);
+    w[d] = ok ? (o == 0 ? 1.f : 0.5f) : 0.f;
+  }
+}
+// Prolongation: a fine node on a coarse node takes it with weight 1, a node
+// between two coarse nodes takes both with weight 1/2.
+__device__ __forceinline__ void prolong_axis(int f, int i, int* idx, float* w) {
+  if (f == 1) { idx[0] = idx[1] = i; w[0] = 1.f; w[1] = 0.f; }
+  else if ((i & 1) == 0) { idx[0] = idx[1] = i / 2; w[0] = 1.f; w[1] = 0.f; }
+  else { idx[0] = (i - 1) / 2; idx[1] = (i + 1) / 2; w[0] = w[1] = 0.5f; }
+}
+
+// rc = P^T tf (masked by the coarse fixed bits), coarse node N, vector r;
+// src = tf of vector r.  27 unconditional loads (weight 0 where unused).
+__device__ __forceinline__ float4 restrict_node(int fxf, int fyf, int fzf, int NXf, int NYf, int NZf, int NXc,
+                                                int NYc, int N, const float* __restrict__ src) {
+  int I, J, K;
+  node_ijk(N, NXc, NYc, I, J, K);
+  int ix[3], iy[3], iz[3];
+  float wx[3], wy[3], wz[3];
+  restrict_axis(fxf, I, NXf, ix, wx);
+  restrict_axis(fyf, J, NYf, iy, wy);
+  restrict_axis(fzf, K, NZf, iz, wz);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int t = 0; t < 27; ++t) {
+    const int a = t % 3, b = (t / 3) % 3, c = t / 9;
+    const float w = wx[a] * wy[b] * wz[c];
+    const int m = (iz[c] * NYf + iy[b]) * NXf + ix[a];
+    const float4 v = __ldg(reinterpret_cast<const float4*>(src) + m);
+    a0 = fmaf(w, v.x, a0); a1 = fmaf(w, v.y, a1); a2 = fmaf(w, v.z, a2);
+  }
+  return make_float4(a0, a1, a2, 0.f);
+}
+
+// (P ec)_n for fine node n, vector r; src = ec of vector r.  8 unconditional loads.
+__device__ __forceinline__ float4 prolong_node(int fx, int fy, int fz, int NXf, int NYf, int NXc, int NYc, int n,
+                                               const float* __restrict__ src) {
+  int i, j, k;
+  node_ijk(n, NXf, NYf, i, j, k);
+  int ix[2], iy[2], iz[2];
+  float wx[2], wy[2], wz[2];
+  prolong_axis(fx, i, ix, wx);
+  prolong_axis(fy, j, iy, wy);
+  prolong_axis(fz, k, iz, wz);
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int a = t & 1, b = (t >> 1) & 1, c = t >> 2;
+    const float w = wx[a] * wy[b] * wz[c];
+    const int m = (iz[c] * NYc + iy[b]) * NXc + ix[a];
+    const float4 v = __ldg(reinterpret_cast<const float4*>(src) + m);
+    a0 = fmaf(w, v.x, a0); a1 = fmaf(w, v.y, a1); a2 = fmaf(w, v.z, a2);
+  }
+  return make_float4(a0, a1, a2, 0.f);
+}
+
 
 // ---------------------------------------------------------------------------
 // Galerkin coarse element matrices
@@ -335,14 +407,17 @@ __global__ void __launch_bounds__(768) k_mgs_op(LevelView L, int R, const float*
   node_ijk(n, L.NX, L.NY, i, j, k);
   const float* xr = x + r * vs;
   const float* S = L.St + (size_t)q * 3 * L.NN + n;
+  int xo[3], yo[3], zo[3];     // clamped neighbour coordinates (their stencil blocks are zero)
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    xo[d] = min(max(i + d - 1, 0), L.NX - 1);
+    yo[d] = min(max(j + d - 1, 0), L.NY - 1) * L.NX;
+    zo[d] = min(max(k + d - 1, 0), L.NZ - 1) * L.NX * L.NY;
+  }
   float acc = 0.f;
 #pragma unroll
   for (int nb = 0; nb < 27; ++nb) {
-    const int dx = nb % 3 - 1, dy = (nb / 3) % 3 - 1, dz = nb / 9 - 1;
-    const bool in = (unsigned)(i + dx) < (unsigned)L.NX && (unsigned)(j + dy) < (unsigned)L.NY &&
-                    (unsigned)(k + dz) < (unsigned)L.NZ;
-    if (!in) continue;
-    const int m = n + (dz * L.NY + dy) * L.NX + dx;
+    const int m = zo[nb / 9] + yo[(nb / 3) % 3] + xo[nb % 3];
     const float4 xv = __ldg(reinterpret_cast<const float4*>(xr) + m);
     const float* Sq = S + (size_t)nb * 9 * L.NN;
     acc = fmaf(__ldg(Sq), xv.x, acc);
@@ -436,32 +511,11 @@ __global__ void k_mg_restrict(Transfer T, int R, const float* __restrict__ tf, c
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)NNc * R) return;
   const int N = int(t % NNc), r = int(t / NNc);
-  int I, J, K;
-  node_ijk(N, T.NXc, T.NYc, I, J, K);
   const long long vsf = (long long)T.NXf * T.NYf * T.NZf * 4, vsc = (long long)NNc * 4;
-  const float4* src = reinterpret_cast<const float4*>(tf + r * vsf);
-  float acc[3] = {0.f, 0.f, 0.f};
-  const int dz0 = T.fz == 2 ? -1 : 0, dz1 = T.fz == 2 ? 1 : 0;
-  const int dy0 = T.fy == 2 ? -1 : 0, dy1 = T.fy == 2 ? 1 : 0;
-  const int dx0 = T.fx == 2 ? -1 : 0, dx1 = T.fx == 2 ? 1 : 0;
-  for (int dk = dz0; dk <= dz1; ++dk) {
-    const int k = T.fz * K + dk;
-    if (k < 0 || k >= T.NZf) continue;
-    for (int dj = dy0; dj <= dy1; ++dj) {
-      const int j = T.fy * J + dj;
-      if (j < 0 || j >= T.NYf) continue;
-      for (int di = dx0; di <= dx1; ++di) {
-        const int i = T.fx * I + di;
-        if (i < 0 || i >= T.NXf) continue;
-        const float w = (dk ? 0.5f : 1.f) * (dj ? 0.5f : 1.f) * (di ? 0.5f : 1.f);
-        const float4 v = __ldg(src + (k * T.NYf + j) * T.NXf + i);
-        acc[0] += w * v.x; acc[1] += w * v.y; acc[2] += w * v.z;
-      }
-    }
-  }
+  const float4 a = restrict_node(T.fx, T.fy, T.fz, T.NXf, T.NYf, T.NZf, T.NXc, T.NYc, N, tf + r * vsf);
   const uint8_t fx = fixc[N];
   reinterpret_cast<float4*>(rc + r * vsc)[N] =
-      make_float4((fx & 1) ? 0.f : acc[0], (fx & 2) ? 0.f : acc[1], (fx & 4) ? 0.f : acc[2], 0.f);
+      make_float4((fx & 1) ? 0.f : a.x, (fx & 2) ? 0.f : a.y, (fx & 4) ? 0.f : a.z, 0.f);
 }
 
 // e_f += P e_c (masked by the fine fixed bits); one thread per (fine node,
@@ -472,33 +526,13 @@ __global__ void k_mg_prolong(Transfer T, int R, const float* __restrict__ ec, co
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= (long long)NNf * R) return;
   const int n = int(t % NNf), r = int(t / NNf);
-  int i, j, k;
-  node_ijk(n, T.NXf, T.NYf, i, j, k);
   const long long vsf = (long long)NNf * 4, vsc = (long long)T.NXc * T.NYc * T.NZc * 4;
-  int Ix[2], Iy[2], Iz[2];
-  float wx[2], wy[2], wz[2];
-  int cx, cy, cz;
-  auto axis = [](int f, int i_, int* I_, float* w_, int& c_) {
-    if (f == 1 || (i_ & 1) == 0) { I_[0] = f == 1 ? i_ : i_ / 2; w_[0] = 1.f; c_ = 1; }
-    else { I_[0] = (i_ - 1) / 2; I_[1] = (i_ + 1) / 2; w_[0] = w_[1] = 0.5f; c_ = 2; }
-  };
-  axis(T.fx, i, Ix, wx, cx);
-  axis(T.fy, j, Iy, wy, cy);
-  axis(T.fz, k, Iz, wz, cz);
-  const float4* src = reinterpret_cast<const float4*>(ec + r * vsc);
-  float acc[3] = {0.f, 0.f, 0.f};
-  for (int c = 0; c < cz; ++c)
-    for (int b = 0; b < cy; ++b)
-      for (int a = 0; a < cx; ++a) {
-        const float w = wx[a] * wy[b] * wz[c];
-        const float4 v = __ldg(src + (Iz[c] * T.NYc + Iy[b]) * T.NXc + Ix[a]);
-        acc[0] += w * v.x; acc[1] += w * v.y; acc[2] += w * v.z;
-      }
+  const float4 a = prolong_node(T.fx, T.fy, T.fz, T.NXf, T.NYf, T.NXc, T.NYc, n, ec + r * vsc);
   const uint8_t fx = fixf[n];
   float4 o = reinterpret_cast<float4*>(ef + r * vsf)[n];
-  if (!(fx & 1)) o.x += acc[0];
-  if (!(fx & 2)) o.y += acc[1];
-  if (!(fx & 4)) o.z += acc[2];
+  if (!(fx & 1)) o.x += a.x;
+  if (!(fx & 2)) o.y += a.y;
+  if (!(fx & 4)) o.z += a.z;
   reinterpret_cast<float4*>(ef + r * vsf)[n] = o;
 }
 
@@ -598,6 +632,8 @@ void mg_destroy(Ctx& c) {
     cudaFree(L.r); cudaFree(L.e); cudaFree(L.e2); cudaFree(L.t);
   }
   for (auto& g : mg->gexec)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto& g : mg->vexec)
     if (g) cudaGraphExecDestroy(g);
   void* ps[] = {mg->A, mg->Y, mg->Ainv, mg->x, mg->r, mg->z, mg->q, mg->p[0], mg->p[1], mg->S, mg->flags, mg->cnt,
                 mg->info, mg->part, mg->omega, mg->lam};
@@ -711,8 +747,7 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-// Apply the V-cycle to mg->L[0].r (R vectors); result in mg->L[0].e.
-int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
+static int vcycle_eager(Ctx& c, int R, cudaStream_t s) {
   if (c.mg->nlev == 1) {
     MGLevel& L = c.mg->L[0];
     k_mg_coarse_solve<<<R, 256, 0, s>>>(L.NN, c.mg->Ainv, L.r, L.e);
@@ -726,6 +761,38 @@ int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
     case 8: return vcycle_t<8>(c, s);
   }
   return -1;
+}
+
+// Apply the V-cycle to mg->L[0].r (R vectors); result in mg->L[0].e.  Inside
+// a stream capture (the PCG graphs) the kernels are recorded as they are;
+// otherwise the cycle for this R is captured once and replayed as a graph,
+// which removes the per-kernel launch overhead of ~40 short launches (the
+// buffers, tensor maps and smoothing weights it references never move).
+int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
+  MG* mg = c.mg;
+  const int ri = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : -1;
+  if (ri < 0) return -1;
+  if (capturing() || mg->vgraph_failed) return vcycle_eager(c, R, s);
+  if (!mg->vexec[ri]) {
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    capturing() = ok;
+    if (ok) ok = vcycle_eager(c, R, s) == 0;
+    capturing() = false;
+    const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
+    if (ok && ended && graph && cudaGraphInstantiate(&mg->vexec[ri], graph, 0) == cudaSuccess) {
+      cudaGraphGetNodes(graph, nullptr, &mg->vnodes[ri]);
+    } else {
+      mg->vexec[ri] = nullptr;
+      mg->vgraph_failed = true;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
+    if (!mg->vexec[ri]) return vcycle_eager(c, R, s);
+  }
+  if (cudaGraphLaunch(mg->vexec[ri], s) != cudaSuccess) return -2;
+  count_launch((long long)mg->vnodes[ri]);
+  return 0;
 }
 
 int mg_query(Ctx& c, int level, int* dims, float* omega, cudaStream_t s) {

@@ -471,6 +471,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   int* info = c.status + 8;
   const int rblocks = 2 * c.num_sms;
   int cur = 0;
+  if (precond == 2 && mg_ensure(c, s)) return -2;
   // X <- X64 (first nb vectors), KX, MX
   launch_convert(X64, true, B.S[cur], f64, (long long)nb * vs, s);
   if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
@@ -639,6 +640,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   cudaMemcpyAsync(hth, th, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
+
   if (hinfo < 0) { c.last_error = "LOBPCG: final block rank deficient"; return -3; }
   for (int j = 0; j < nmodes; ++j) lam[j] = hth[j];
   return conv ? 0 : 1;
