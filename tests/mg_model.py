@@ -1,7 +1,7 @@
 """NumPy model of the library's multigrid hierarchy (test helper).
 
 Same coarsening rule (each axis with >= 2 elements halves, ceil; axes of one
-element are kept; stop at <= 64 nodes) and the same trilinear prolongation,
+element are kept; stop at <= 160 nodes) and the same trilinear prolongation,
 so the device's Galerkin coarse operators can be checked against an explicit
 P^T (D K D) P built from the oracle's assembled stiffness.
 """
@@ -9,7 +9,7 @@ import numpy as np
 import scipy.sparse as sp
 
 
-def levels(nx, ny, nz, cap=64):
+def levels(nx, ny, nz, cap=160):
     L = [(nx, ny, nz, 1, 1, 1)]
     while True:
         nx, ny, nz = L[-1][:3]

@@ -27,13 +27,44 @@ def oracle_for(name, g):
 
 
 @pytest.mark.parametrize("name", ["tiny", "cantilever"])
-def test_hierarchy_and_galerkin(golden, name):
+def test_hierarchy(golden, name):
     g = golden(name)
     ctx = make_ctx(g, g["rho"])
     lv = ctx.mg_levels()
     expect = levels(int(g["nx"]), int(g["ny"]), int(g["nz"]))
     assert [l[:3] for l in lv] == [e[:3] for e in expect]
     assert all(0.0 < l[3] < 0.6 for l in lv[:-1])          # 1.33 / lambda_max, lambda ~ 3.5..4.5
+
+
+def test_single_level_is_exact_coarse_solve(golden):
+    """A grid at or below the coarsest-level size is one level: the V-cycle is
+    the dense FP64 inverse, so mg_apply(r) = K_ff^-1 r (FP32 in and out)."""
+    import scipy.sparse.linalg as spla
+    g = golden("tiny")
+    ctx = make_ctx(g, g["rho"])
+    assert len(ctx.mg_levels()) == 1
+    fem = oracle_for("tiny", g)
+    K = fem.assemble_K(g["rho"]).tocsr()
+    fd = fem.free_dofs
+    rng = np.random.default_rng(3)
+    r = np.zeros((2, K.shape[0]))
+    r[:, fd] = rng.standard_normal((2, len(fd)))
+    r32 = ctx.pack(to_dev(r), dtype=torch.float32)
+    e = ctx.unpack(ctx.mg_apply(r32).double()).cpu().numpy()
+    rq = ctx.unpack(r32.double()).cpu().numpy()            # the FP32-rounded right-hand sides
+    Kff = K[fd][:, fd].tocsc()
+    for k in range(2):
+        ref = spla.spsolve(Kff, rq[k, fd])
+        assert rel(e[k, fd], ref) < 1e-5
+        assert np.all(e[k, np.setdiff1d(np.arange(K.shape[0]), fd)] == 0.0)
+
+
+def test_galerkin_level1(golden):
+    name = "cantilever"
+    g = golden(name)
+    ctx = make_ctx(g, g["rho"])
+    expect = levels(int(g["nx"]), int(g["ny"]), int(g["nz"]))
+    assert len(expect) >= 2
     fem = oracle_for(name, g)
     K = fem.assemble_K(g["rho"]).tocsr()
     free = np.zeros(K.shape[0])

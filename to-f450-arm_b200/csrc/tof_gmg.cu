@@ -31,7 +31,7 @@
 
 namespace tof {
 
-constexpr int kCoarseNodes = 64;
+constexpr int kCoarseNodes = 160;
 constexpr int kMaxLevels = 10;
 // Jacobi smoothing weight omega = kOmegaScale / lambda_max(D^-1 A).  4/3 is
 // the classical high-frequency-optimal choice; a 10-step power iteration
@@ -302,12 +302,16 @@ __global__ void k_mg_stencil(int nx, int ny, int nz, const float* __restrict__ A
   for (int e = 0; e < 9; ++e) St[(size_t)(nb * 9 + e) * NN + n] = float(s[e]);
 }
 
-// Coarsest level: dense assembly (row per thread), Cholesky, inverse.
-// Level 0 (Ae == null) assembles from factors and Ke with the fixed mask.
-__global__ void __launch_bounds__(256) k_mg_coarse_setup(int nx, int ny, int nz, const float* __restrict__ Ae,
+constexpr int kCholB = 16;   // Cholesky panel width
+static size_t coarse_setup_smem(int n) { return sizeof(double) * (kCholB + 1) * (kCholB + n); }
+
+// Coarsest level: dense assembly (row per thread) and blocked Cholesky in one
+// CTA; the inverse is formed by k_mg_coarse_inverse.  Level 0 (Ae == null)
+// assembles from factors and Ke with the fixed mask.
+__global__ void __launch_bounds__(1024) k_mg_coarse_setup(int nx, int ny, int nz, const float* __restrict__ Ae,
                                                          const double* __restrict__ fK, const double* __restrict__ Ke,
                                                          const uint8_t* __restrict__ fix, double* A, double* Y,
-                                                         double* Ainv, int* info) {
+                                                         int* info) {
   const int NX = nx + 1, NY = ny + 1, NZ = nz + 1, NN = NX * NY * NZ, n = 3 * NN;
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) A[i] = 0.0;
   __syncthreads();
@@ -339,45 +343,142 @@ __global__ void __launch_bounds__(256) k_mg_coarse_setup(int nx, int ny, int nz,
     if (fixed_row) A[(size_t)row * n + row] = 1.0;
   }
   __syncthreads();
-  // Cholesky (lower, in place)
+  // Blocked right-looking Cholesky A = L L^T (lower triangle, in place),
+  // panels of kCholB columns: (1) one warp factors the diagonal block in
+  // shared memory, (2) each row below solves against it (thread per row) and
+  // the panel is kept in shared memory, (3) the trailing lower triangle is
+  // updated once per panel (warp per row, lanes over columns), so A makes
+  // n / kCholB passes through L2 instead of n.
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  extern __shared__ double sh[];
+  constexpr int LD = kCholB + 1;
+  double* Dg = sh;                     // [kCholB][LD] diagonal block
+  double* Pn = sh + kCholB * LD;       // [rows below][LD] panel
   __shared__ int s_bad;
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
-  for (int kk = 0; kk < n; ++kk) {
-    if (threadIdx.x == 0) {
-      const double d = A[(size_t)kk * n + kk];
-      if (!(d > 0.0)) { s_bad = kk + 1; A[(size_t)kk * n + kk] = 1.0; }
-      else A[(size_t)kk * n + kk] = sqrt(d);
+  for (int kb = 0; kb < n; kb += kCholB) {
+    const int w = min(kCholB, n - kb);
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x)
+      Dg[(e / w) * LD + e % w] = A[(size_t)(kb + e / w) * n + kb + e % w];
+    __syncthreads();
+    if (warp == 0) {
+      for (int t = 0; t < w; ++t) {
+        if (lane == 0) {
+          double d = Dg[t * LD + t];
+          if (!(d > 0.0)) { s_bad = kb + t + 1; d = 1.0; }
+          Dg[t * LD + t] = sqrt(d);
+        }
+        __syncwarp();
+        const double ip = 1.0 / Dg[t * LD + t];
+        if (lane > t && lane < w) Dg[lane * LD + t] *= ip;
+        __syncwarp();
+        if (lane > t && lane < w)
+          for (int c2 = t + 1; c2 <= lane; ++c2) Dg[lane * LD + c2] -= Dg[lane * LD + t] * Dg[c2 * LD + t];
+        __syncwarp();
+      }
     }
     __syncthreads();
-    const double piv = A[(size_t)kk * n + kk];
-    for (int i = kk + 1 + threadIdx.x; i < n; i += blockDim.x) A[(size_t)i * n + kk] /= piv;
-    __syncthreads();
-    const int m = n - kk - 1;
-    for (int w = threadIdx.x; w < m * m; w += blockDim.x) {
-      const int i = kk + 1 + w / m, j = kk + 1 + w % m;
-      if (j <= i) A[(size_t)i * n + j] -= A[(size_t)i * n + kk] * A[(size_t)j * n + kk];
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+      const int r0 = e / w, c0 = e % w;
+      if (c0 <= r0) {
+        A[(size_t)(kb + r0) * n + kb + c0] = Dg[r0 * LD + c0];
+        A[(size_t)(kb + c0) * n + kb + r0] = Dg[r0 * LD + c0];
+      }
+      if (c0 == r0) Y[kb + r0] = 1.0 / Dg[r0 * LD + r0];
+    }
+    const int base = kb + w;
+    for (int i = base + threadIdx.x; i < n; i += blockDim.x) {
+      double x[kCholB];
+#pragma unroll
+      for (int t = 0; t < kCholB; ++t) x[t] = t < w ? A[(size_t)i * n + kb + t] : 0.0;
+#pragma unroll
+      for (int t = 0; t < kCholB; ++t) {
+        if (t < w) {
+#pragma unroll
+          for (int u = 0; u < t; ++u) x[t] = fma(-x[u], Dg[t * LD + u], x[t]);
+          x[t] /= Dg[t * LD + t];
+          A[(size_t)i * n + kb + t] = x[t];
+          A[(size_t)(kb + t) * n + i] = x[t];      // L^T in the upper triangle
+          Pn[(i - base) * LD + t] = x[t];
+        }
+      }
     }
     __syncthreads();
-  }
-  // Y = L^-1 (column j by thread j)
-  for (int jc = threadIdx.x; jc < n; jc += blockDim.x) {
-    for (int i = 0; i < n; ++i) {
-      double s = (i == jc) ? 1.0 : 0.0;
-      for (int kk = jc; kk < i; ++kk) s -= A[(size_t)i * n + kk] * Y[(size_t)kk * n + jc];
-      Y[(size_t)i * n + jc] = i < jc ? 0.0 : s / A[(size_t)i * n + i];
+    for (int i = base + warp; i < n; i += nwarps) {
+      double pi[kCholB];
+#pragma unroll
+      for (int t = 0; t < kCholB; ++t) pi[t] = t < w ? Pn[(i - base) * LD + t] : 0.0;
+      for (int j = base + lane; j <= i; j += 32) {
+        const double* pj = Pn + (j - base) * LD;
+        double sum = 0.0;
+#pragma unroll
+        for (int t = 0; t < kCholB; ++t) sum = fma(pi[t], t < w ? pj[t] : 0.0, sum);
+        A[(size_t)i * n + j] -= sum;
+      }
     }
-  }
-  __syncthreads();
-  // Ainv = Y^T Y, zero on fixed DOFs
-  for (int w = threadIdx.x; w < n * n; w += blockDim.x) {
-    const int i = w / n, j = w % n;
-    double s = 0.0;
-    for (int kk = max(i, j); kk < n; ++kk) s += Y[(size_t)kk * n + i] * Y[(size_t)kk * n + j];
-    const bool fi = (fix[i / 3] >> (i % 3)) & 1, fj = (fix[j / 3] >> (j % 3)) & 1;
-    Ainv[w] = (fi || fj) ? 0.0 : s;
+    __syncthreads();
   }
   if (threadIdx.x == 0) info[0] = s_bad;
+}
+
+// Coarsest inverse from the Cholesky factor: one warp per column j of
+// A^-1 = L^-T L^-1.  The column lives in registers (lane l holds entries
+// l + 32 m); the forward solve L y = e_j and the back solve L^T x = y run in
+// axpy form, so each step is one shuffle broadcast plus coalesced loads of a
+// row of L^T (forward) or of L (backward) -- no long dependent dot products.
+// LLt: L in the lower and L^T in the upper triangle; idg[k] = 1 / L[k][k].
+// The result is written as row j (A^-1 is symmetric); rows and columns of
+// fixed DOFs are zero.
+constexpr int kInvSlots = (3 * kCoarseNodes + 31) / 32;
+__global__ void __launch_bounds__(256) k_mg_coarse_inverse(int n, const double* __restrict__ LLt,
+                                                           const double* __restrict__ idg,
+                                                           const uint8_t* __restrict__ fix, double* Ainv) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (j >= n) return;
+  double y[kInvSlots];
+#pragma unroll
+  for (int m = 0; m < kInvSlots; ++m) y[m] = (lane + 32 * m == j) ? 1.0 : 0.0;
+  // forward: for k = j .. n-1: y_k /= L_kk; y_i -= L_ik y_k (i > k)
+  for (int k = j; k < n; ++k) {
+    double own = 0.0;
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m)
+      if (m == (k >> 5)) own = y[m];
+    const double yk = __shfl_sync(0xffffffffu, own, k & 31) * idg[k];
+    const double* col = LLt + (size_t)k * n;          // L^T row k = L column k
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m) {
+      const int i = lane + 32 * m;
+      if (i == k) y[m] = yk;
+      else if (i > k && i < n) y[m] = fma(-col[i], yk, y[m]);
+    }
+  }
+  // backward: for k = n-1 .. 0: x_k = y_k / L_kk; y_i -= L_ki x_k (i < k)
+  for (int k = n - 1; k >= 0; --k) {
+    double own = 0.0;
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m)
+      if (m == (k >> 5)) own = y[m];
+    const double xk = __shfl_sync(0xffffffffu, own, k & 31) * idg[k];
+    const double* row = LLt + (size_t)k * n;          // L row k (lower part)
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m) {
+      const int i = lane + 32 * m;
+      if (i == k) y[m] = xk;
+      else if (i < k) y[m] = fma(-row[i], xk, y[m]);
+    }
+  }
+  const bool fj = (fix[j / 3] >> (j % 3)) & 1;
+#pragma unroll
+  for (int m = 0; m < kInvSlots; ++m) {
+    const int i = lane + 32 * m;
+    if (i < n) {
+      const bool fi = (fix[i / 3] >> (i % 3)) & 1;
+      Ainv[(size_t)j * n + i] = (fi || fj) ? 0.0 : y[m];
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -536,23 +637,48 @@ __global__ void k_mg_prolong(Transfer T, int R, const float* __restrict__ ec, co
   reinterpret_cast<float4*>(ef + r * vsf)[n] = o;
 }
 
-// coarsest: e = Ainv r, one CTA per right-hand side (n <= 3 * kCoarseNodes).
-// Ainv is symmetric, so row i is read as column i: consecutive threads read
-// consecutive addresses.
-__global__ void __launch_bounds__(256) k_mg_coarse_solve(int NN, const double* __restrict__ Ainv,
-                                                         const float* __restrict__ r, float* e) {
-  __shared__ double sr[3 * kCoarseNodes];
+// coarsest: e = Ainv r (n = 3 NN <= 3 * kCoarseNodes per vector, R <= 8
+// right-hand sides).  Every CTA stages all right-hand sides in shared memory;
+// one warp per row i reads row i of Ainv coalesced (lanes over columns),
+// accumulates the R products and reduces them with shuffles.
+constexpr int kCoarseWarps = 8;
+__global__ void __launch_bounds__(32 * kCoarseWarps) k_mg_coarse_solve(int NN, int R, const double* __restrict__ Ainv,
+                                                                       const float* __restrict__ r, float* e) {
+  __shared__ double sr[TOF_MAX_RHS][3 * kCoarseNodes];
   const int n = 3 * NN;
-  const float* rr = r + (size_t)blockIdx.x * NN * 4;
-  float* er = e + (size_t)blockIdx.x * NN * 4;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) sr[i] = double(rr[(i / 3) * 4 + i % 3]);
-  __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double s = 0.0;
-    for (int j = 0; j < n; ++j) s = fma(Ainv[(size_t)j * n + i], sr[j], s);
-    er[(i / 3) * 4 + i % 3] = float(s);
+  for (int w = threadIdx.x; w < R * n; w += blockDim.x) {
+    const int q = w / n, i = w % n;
+    sr[q][i] = double(r[(size_t)q * NN * 4 + (i / 3) * 4 + i % 3]);
   }
-  for (int i = threadIdx.x; i < NN; i += blockDim.x) er[i * 4 + 3] = 0.f;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kCoarseWarps + (threadIdx.x >> 5);
+  if (i >= n) return;
+  double acc[TOF_MAX_RHS];
+#pragma unroll
+  for (int q = 0; q < TOF_MAX_RHS; ++q) acc[q] = 0.0;
+  const double* row = Ainv + (size_t)i * n;
+  for (int j = lane; j < n; j += 32) {
+    const double a = row[j];
+#pragma unroll
+    for (int q = 0; q < TOF_MAX_RHS; ++q)
+      if (q < R) acc[q] = fma(a, sr[q][j], acc[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < TOF_MAX_RHS; ++q) {
+    if (q >= R) break;
+    const double v = warp_sum(acc[q]);
+    if (lane == 0) {
+      float* er = e + (size_t)q * NN * 4;
+      er[(i / 3) * 4 + i % 3] = float(v);
+      if (i % 3 == 0) er[(i / 3) * 4 + 3] = 0.f;
+    }
+  }
+}
+
+static void launch_coarse_solve(int NN, int R, const double* Ainv, const float* r, float* e, cudaStream_t s) {
+  k_mg_coarse_solve<<<ceil_div(3 * NN, kCoarseWarps), 32 * kCoarseWarps, 0, s>>>(NN, R, Ainv, r, e);
+  count_launch();
 }
 
 // ---------------------------------------------------------------------------
@@ -666,8 +792,12 @@ int mg_setup(Ctx& c, cudaStream_t s) {
     }
   }
   const MGLevel& L = mg->L[mg->nlev - 1];
-  k_mg_coarse_setup<<<1, 256, 0, s>>>(L.nx, L.ny, L.nz, mg->nlev > 1 ? L.Ae : nullptr, c.fK64, c.Ke64, L.fix, mg->A,
-                                      mg->Y, mg->Ainv, mg->info);
+  const size_t csm = coarse_setup_smem(mg->nc);
+  cudaFuncSetAttribute(k_mg_coarse_setup, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+  k_mg_coarse_setup<<<1, 1024, csm, s>>>(L.nx, L.ny, L.nz, mg->nlev > 1 ? L.Ae : nullptr, c.fK64, c.Ke64, L.fix, mg->A,
+                                      mg->Y, mg->info);
+  count_launch();
+  k_mg_coarse_inverse<<<ceil_div(mg->nc, 8), 256, 0, s>>>(mg->nc, mg->A, mg->Y, L.fix, mg->Ainv);
   count_launch();
   // smoothing weights: power iteration on D^-1 A_l (scratch: the level's e, e2)
   for (int k = 0; k < mg->nlev - 1; ++k) {
@@ -727,8 +857,7 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
   }
   {
     MGLevel& L = mg->L[nl - 1];
-    k_mg_coarse_solve<<<R, 256, 0, s>>>(L.NN, mg->Ainv, L.r, L.e);
-    count_launch();
+    launch_coarse_solve(L.NN, R, mg->Ainv, L.r, L.e, s);
     cur[nl - 1] = L.e;
   }
   // upward
@@ -750,8 +879,7 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
 static int vcycle_eager(Ctx& c, int R, cudaStream_t s) {
   if (c.mg->nlev == 1) {
     MGLevel& L = c.mg->L[0];
-    k_mg_coarse_solve<<<R, 256, 0, s>>>(L.NN, c.mg->Ainv, L.r, L.e);
-    count_launch();
+    launch_coarse_solve(L.NN, R, c.mg->Ainv, L.r, L.e, s);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
   }
   switch (R) {

@@ -204,24 +204,42 @@ __device__ bool warp_syev(double (*A)[LDA], double (*Q)[LDA], double* d, EigScra
 // In-place Cholesky B = L L^T of a symmetric n x n matrix (lower triangle
 // and diagonal become L); idiag[k] = 1 / L[k][k].  false (uniformly across
 // the warp) when a pivot is not above piv_min: the basis is too close to
-// dependent for Cholesky-based orthonormalisation.
+// dependent for Cholesky-based orthonormalisation.  Lane i keeps row i in
+// registers; column k is broadcast with shuffles.
 __device__ bool warp_chol(double (*B)[LDA], double* idiag, int n, double piv_min) {
   const int lane = threadIdx.x;
-  for (int k = 0; k < n; ++k) {
-    const double pk = B[k][k];
-    if (!(pk > piv_min)) return false;
-    const double ir = rsqrt(pk);
-    __syncwarp();
-    if (lane > k && lane < n) B[lane][k] *= ir;
-    if (lane == k) { B[k][k] = pk * ir; idiag[k] = ir; }
-    __syncwarp();
-    if (lane > k && lane < n) {
-      const double lik = B[lane][k];
-      for (int j = k + 1; j <= lane; ++j) B[lane][j] -= lik * B[j][k];
+  const unsigned full = 0xffffffffu;
+  constexpr int NB = kMaxBasis;
+  double b[NB];
+#pragma unroll
+  for (int j = 0; j < NB; ++j) b[j] = (lane < n && j < n) ? B[lane][j] : 0.0;
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < NB; ++k) {
+    if (k < n && ok) {
+      const double pk = __shfl_sync(full, b[k], k);
+      if (!(pk > piv_min)) {
+        ok = false;
+      } else {
+        const double ir = rsqrt(pk);
+        if (lane == k) { b[k] = pk * ir; if (lane < NB) idiag[k] = ir; }
+        else if (lane > k) b[k] *= ir;
+        const double lik = b[k];
+#pragma unroll
+        for (int j = k + 1; j < NB; ++j) {
+          const double ljk = __shfl_sync(full, b[k], j);
+          if (lane > k && j <= lane && j < n) b[j] = fma(-lik, ljk, b[j]);
+        }
+      }
     }
-    __syncwarp();
   }
-  return true;
+  if (ok && lane < n) {
+#pragma unroll
+    for (int j = 0; j < NB; ++j)
+      if (j <= lane && j < n) B[lane][j] = b[j];
+  }
+  __syncwarp();
+  return ok;
 }
 
 // Rayleigh-Ritz: the m smallest eigenpairs of G_K c = theta G_M c (n x n).
