@@ -413,14 +413,27 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       st[k] = sk;
     }
   } else if (mode == TOF_MODE_MIXED) {
-    // FP64 PCG preconditioned by the FP32 multigrid V-cycle
+    // FP64 PCG preconditioned by the FP32 multigrid V-cycle.  The recursive
+    // residual drifts from the true one (by ~eps * cond); when it claims
+    // convergence but the true residual b - K x does not meet rtol, the
+    // iteration restarts from the current x (a restart recomputes r in FP64),
+    // at most kMaxRestarts times.
+    constexpr int kMaxRestarts = 4;
     int ist[8] = {0};
-    if (pcg_mg64(c, wb, wx, R, rtol, maxiter, iters, ist, s)) return TOF_ERR_CUDA;
-    if (true_relres(c, wb, wx, R, rel, s)) return TOF_ERR_CUDA;
-    for (int k = 0; k < nrhs; ++k) {
-      outer[k] = 1;
-      st[k] = ist[k];
-      if (st[k] == ST_OK && rel[k] > rtol * 1.01) st[k] = ST_NOT_CONVERGED;
+    for (int o = 0; o <= kMaxRestarts; ++o) {
+      int it_o[8] = {0};
+      const int budget = maxiter - *std::max_element(iters, iters + R);
+      if (budget <= 0) break;
+      if (pcg_mg64(c, wb, wx, R, rtol, budget, it_o, ist, s)) return TOF_ERR_CUDA;
+      if (true_relres(c, wb, wx, R, rel, s)) return TOF_ERR_CUDA;
+      bool again = false;
+      for (int k = 0; k < nrhs; ++k) {
+        iters[k] += it_o[k];
+        outer[k] = o + 1;
+        st[k] = ist[k];
+        if (st[k] == ST_OK && rel[k] > rtol * 1.01) { st[k] = ST_NOT_CONVERGED; again = true; }
+      }
+      if (!again) break;
     }
   } else {
     // FP64 iterative refinement around the FP32 standard PCG

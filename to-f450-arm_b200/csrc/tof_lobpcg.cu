@@ -2,20 +2,22 @@
 //
 // The reference calls SciPy's lobpcg on the assembled K_ff, M_ff with a Jacobi
 // preconditioner, tol 1e-4, maxiter 500 (src/fem.py:400-470; CuPy's lobpcg
-// on the GPU, src/fem_gpu.py:101-173).  Here the block vectors live on the
-// device in node4 layout; each iteration:
-//   W = K X - M X diag(theta)           (k_lob_resid, FP64 norms)
-//   W <- T W                            (Jacobi, or a few pipelined block-PCG
-//                                        iterations on K: inexact K^-1)
+// on the GPU, src/fem_gpu.py:101-173).  Here the FP64 block vectors live on
+// the device in node4 layout; each iteration:
+//   W = K X - M X diag(theta)           (k_lob_resid, FP64 norms; soft-locked
+//                                        columns leave W)
+//   W <- T W                            (Jacobi, a few FP32 PCG iterations,
+//                                        or one FP32 multigrid V-cycle)
 //   KW, MW                              (matrix-free block matvecs)
-//   G_K = S^T K S, G_M = S^T M S        (S = [X W P], FP64 Gram)
-//   Rayleigh-Ritz on (G_K, G_M)         (k_small_eig: one warp, FP64 Jacobi,
-//                                        basis conditioning by eigen-
-//                                        decomposition of the scaled G_M)
+//   G_K = S^T K S, G_M = S^T M S        (S = [X W_act P_act], FP64 Gram)
+//   Rayleigh-Ritz on (G_K, G_M)         (k_small_eig: one warp; Cholesky of
+//                                        the scaled G_M, or SVQB when the
+//                                        basis is ill-conditioned; implicit
+//                                        symmetric QR for the small problem)
 //   X, P, KX, MX, KP, MP <- S C         (k_lob_update)
-// In mixed mode the block vectors are FP32 and a final FP64 Rayleigh-Ritz on
-// freshly computed FP64 K X, M X gives the eigenvalues; in FP64 mode
-// everything is FP64.
+// K X, M X, K P, M P are recomputed every kLobRefresh iterations and before
+// convergence is accepted; a final FP64 Rayleigh-Ritz on fresh products gives
+// the returned pairs.
 #include <math.h>
 #include <stdio.h>
 
@@ -29,6 +31,13 @@ constexpr int kMaxBasis = 24;
 #define TOF_LOB_REFRESH 10
 #endif
 constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M products
+// Below its rounding floor (~eps * lambda_max / lambda_1 of the pencil) the
+// iteration stops converging and its basis can degrade.  The best iterate
+// (smallest worst wanted residual) is kept aside; the iteration stops, not
+// converged, when the residual grows kLobDiverge-fold over that best or has
+// not improved for kLobStall iterations, and the best iterate is returned.
+constexpr int kLobStall = 500;
+constexpr double kLobDiverge = 1e3;
 
 // ---------------------------------------------------------------------------
 // residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, written to
@@ -562,6 +571,11 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     }
     return 0;
   };
+  double best = INFINITY;
+  double best_res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int it_best = 0;
+  bool use_best = false;
+  double* X6 = c.lw64;                         // holds the best iterate (free until the final step)
   for (it = 0; it < maxiter; ++it) {
     const bool fresh = it > 0 && it % kLobRefresh == 0;
     if (fresh && refresh()) return -2;
@@ -586,6 +600,15 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (changed) {                             // W of the new active set
       na = active_map();
       if (residual()) return -2;
+    }
+    if (worst < best) {
+      best = worst;
+      it_best = it;
+      for (int j = 0; j < nmodes; ++j) best_res[j] = rres[j];
+      cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+    } else if (worst > kLobDiverge * best || it - it_best >= kLobStall) {
+      use_best = true;
+      break;
     }
 #ifdef TOF_LOB_TRACE
     fprintf(stderr, "lobpcg it %d rank %d active %d fresh %d worst %.3e res", it, hinfo, na, int(fresh), worst);
@@ -634,12 +657,14 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     cur ^= 1;
   }
   if (iters_out) *iters_out = it;
-  // final FP64 Rayleigh-Ritz on fresh FP64 products
-  double* X6 = c.lw64;
+  if (!conv && it >= maxiter && worst > best) use_best = true;
+  if (use_best && resid_out)
+    for (int j = 0; j < nmodes; ++j) resid_out[j] = best_res[j];
+  // final FP64 Rayleigh-Ritz on fresh FP64 products of X6 (the best iterate,
+  // or the current one)
   double* KX6 = c.lw64 + (long long)c.max_modes * vs;
   double* MX6 = c.lw64 + 2LL * c.max_modes * vs;
-  if (!f64) launch_convert(B.S[cur], false, X6, true, (long long)nb * vs, s);
-  else cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+  if (!use_best) cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
   if (launch_matvec(c, 0, true, X6, KX6, nb, nullptr, s)) return -2;
   if (launch_matvec(c, 1, true, X6, MX6, nb, nullptr, s)) return -2;
   launch_gram(c, true, X6, nb, KX6, nb, GK, s);
