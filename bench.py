@@ -222,6 +222,23 @@ def solver_comparison(torch, L, C):
     return out
 
 
+def reduce_max(x: float, torch, device) -> float:
+    """Max of a per-rank scalar over all ranks (a replica job is as fast as
+    its slowest rank); the value itself on a single process."""
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return x
+    if torch.distributed.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world: int, steps: int, max_total_s: float) -> float:
+    """Whole-job throughput of N independent replicas: N * steps / max time."""
+    return world * steps / max_total_s
+
+
 def own_arm(a, rank, world, local_rank):
     import torch
     from tof_b200 import _lib as L
@@ -249,13 +266,11 @@ def own_arm(a, rank, world, local_rank):
     total, per = time_steps(opt.step, a.steps, flush, torch)
     launches = lib.tof_launch_count() - n0
     torch.cuda.synchronize()
+    total = reduce_max(total, torch, "cuda")
     if world > 1:
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total = float(t.item())
         torch.distributed.barrier()
     clocks = sampler.stop() if sampler else None
-    value = world * a.steps / total
+    value = replica_value(world, a.steps, total)
     hist = opt.history
 
     if a.no_e2e:
@@ -282,11 +297,8 @@ def own_arm(a, rank, world, local_rank):
 
     n_e2e = max(1, min(a.steps, 5))
     e2e_total, _ = time_steps(e2e_step, n_e2e, flush, torch)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e = {"value": world * n_e2e / e2e_total, "unit": "iter/s",
+    e2e_total = reduce_max(e2e_total, torch, "cuda")
+    e2e = {"value": replica_value(world, n_e2e, e2e_total), "unit": "iter/s",
            "h2d_bytes_per_step": int(n_design * 8 + F_host.numel() * 8),
            "d2h_bytes_per_step": int(n_design * 8 + 8 * 4)}
 
