@@ -197,6 +197,36 @@ int tof_eig_sens(tof_ctx* ctx, const double* qK, const double* qM, double lam, d
  * Synchronises `stream`. */
 int tof_effective_mass(tof_ctx* ctx, const double* modes, int nmodes, int direction, double* out, void* stream);
 
+/* Element stress at the element centres for nvec node4 displacement vectors
+ * (dtype TOF_F32 / TOF_F64): sigma_e = rho_e D B_c u_e with the reference's
+ * linear density scaling (FEM3D.compute_stress, src/fem.py:564-579).  B_c:
+ * host 6x24 strain-displacement matrix at the centre (src/fem.py:153-176),
+ * D: host 6x6 elasticity matrix, both row-major, Voigt order xx yy zz xy yz
+ * xz.  rho: device FP64 [NE] over the full grid, or NULL for the density set
+ * by tof_set_density.  Outputs, device FP64 over the full grid (x fastest,
+ * 0 on inactive voxels), each may be NULL: sigma [nvec][NE][6], vm
+ * [nvec][NE] (FEM3D.von_mises, src/fem.py:582-589), smax [nvec][NE]
+ * (FEM3D.principal_stress_max, src/fem.py:592-602). */
+int tof_stress(tof_ctx* ctx, const double* B_c, const double* D, int dtype, const void* u, int nvec,
+               const double* rho, double* sigma, double* vm, double* smax, void* stream);
+
+/* von Mises and largest principal stress of n Voigt stress rows (device FP64
+ * [n][6]; outputs device FP64 [n], either may be NULL).  src/fem.py:582-602. */
+int tof_stress_invariants(long long n, const double* sigma, double* vm, double* smax, void* stream);
+
+/* Fatigue field of a cycle between two stress levels s1, s2 (Pa, device FP64
+ * [n], e.g. the von Mises stresses of two load cases): mean and alternating
+ * stress, Goodman-equivalent alternating stress for ultimate strength
+ * sigma_uts, life from the PA12 S-N curve, damage per cycle and factor of
+ * safety s_design_pa / equivalent stress (fatigue_life_field,
+ * src/fatigue.py:83-112).  out: device FP64 [6][n] in that order. */
+int tof_fatigue(long long n, const double* s1, const double* s2, double sigma_uts, double s_design_pa, double* out,
+                void* stream);
+
+/* Cycles to failure at n equivalent fully reversed stresses (Pa, device FP64)
+ * from the PA12 S-N curve (sn_life, src/fatigue.py:24-65). */
+int tof_sn_life(long long n, const double* sigma_eq, double* life, void* stream);
+
 /* Density filter on an nx*ny*nz element grid (x fastest) with a (kx,ky,kz)
  * weight array (z slowest: w[(qz*ky + qy)*kx + qx], odd sizes) and a mask
  * (NE bytes).  Replaces topopt.cone_kernel / filter_field

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference source tree (read-only):
 
-    python tests/golden/make_golden.py --ref /root/reference [--skip-arm]
+    python tests/golden/make_golden.py --ref /root/reference [--skip-arm] [--only stress]
 
 The reference (NinhGhoster/TO-F450-arm, pure Python + SciPy) is imported from
 its own `src/` and `sims/` packages and driven with the synthetic geometries of
@@ -227,16 +227,51 @@ def make_arm(rfem, rmp):
                 freqs=freqs, lam=lam, eff=eff, umax=np.abs(u).max())
 
 
+def make_stress(rfem):
+    """Element stress (src/fem.py:564-602) on the tiny domain for both load
+    cases, and the Goodman / S-N fatigue field (src/fatigue.py:24-112) on the
+    von Mises pair plus a sweep that reaches every branch of sn_life."""
+    from src import fatigue as rfat
+    g = tiny_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    rng = np.random.default_rng(1)
+    rho = rng.uniform(0.03, 1.0, fem.n_active)
+    rho[:3] = [0.05, 0.1, 0.0999]
+    K = fem.assemble_K(rho)
+    out = dict(rho=rho, B_centre=fem.B_centre, D=fem.D_solid)
+    for i, F in enumerate((g.load_vector(F=(0.0, 0.0, -5.0)), g.load_vector(F=(0.0, 3.0, 1.0), Mz=0.05)), 1):
+        u = fem.apply_BCs_and_solve(K, F, method="lu")
+        sig = fem.compute_stress(u, rho)
+        out[f"u{i}"] = u
+        out[f"sigma{i}"] = sig
+        out[f"vm{i}"] = fem.von_mises(sig)
+        out[f"smax{i}"] = fem.principal_stress_max(sig)
+    # fatigue: stresses in Pa spanning below endurance .. static overload
+    a = rng.uniform(0.0, 90e6, 400)
+    b = rng.uniform(0.0, 90e6, 400)
+    a[:4] = [0.0, 11.9e6, 12.0e6, 30e6]
+    b[:4] = [0.0, 0.0, 5e6, 30e6]
+    fat = rfat.fatigue_life_field(a, b, C.PA12.sigma_u)
+    out.update(fat_s1=a, fat_s2=b, **{f"fat_{k}": v for k, v in fat.items()})
+    out["sn_alt_1e6"] = rfat.sn_alt_stress_at(1e6)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--skip-arm", action="store_true")
+    ap.add_argument("--only", default=None, help="write just this fixture (e.g. stress)")
     a = ap.parse_args()
     rfem, rtop, rmp = setup_reference(a.ref)
+    if a.only == "stress":
+        np.savez_compressed(os.path.join(HERE, "stress.npz"), **make_stress(rfem))
+        return
     np.savez_compressed(os.path.join(HERE, "tiny.npz"), **make_tiny(rfem, rtop, rmp))
     np.savez_compressed(os.path.join(HERE, "oc.npz"), **make_oc(rtop))
     np.savez_compressed(os.path.join(HERE, "simp_small.npz"), **make_simp(rfem, rtop))
     np.savez_compressed(os.path.join(HERE, "cantilever.npz"), **make_cantilever(rfem, rmp))
+    np.savez_compressed(os.path.join(HERE, "stress.npz"), **make_stress(rfem))
     if not a.skip_arm:
         np.savez_compressed(os.path.join(HERE, "arm.npz"), **make_arm(rfem, rmp))
 

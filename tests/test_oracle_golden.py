@@ -151,3 +151,22 @@ def test_arm_inputs(golden):
     K = fem.reduce(fem.assemble_K(g["rho"]))
     assert K.shape[0] == len(g["free_dofs"])
     assert np.all(K.diagonal() > 0)
+
+
+def test_oracle_stress_and_fatigue(golden):
+    """The stress / fatigue restatement reproduces the reference's own outputs."""
+    from oracle import stress as S
+    d = golden("stress")
+    t = golden("tiny")
+    B = S.B_centre(*t["h"])
+    assert np.array_equal(B, d["B_centre"])
+    for i in (1, 2):
+        sig = S.compute_stress(d[f"u{i}"], t["elem_dof_ids"], B, d["D"], d["rho"])
+        np.testing.assert_allclose(sig, d[f"sigma{i}"], rtol=1e-13, atol=1e-13 * np.abs(sig).max())
+        np.testing.assert_allclose(S.von_mises(sig), d[f"vm{i}"], rtol=1e-13)
+        np.testing.assert_allclose(S.principal_stress_max(sig), d[f"smax{i}"], rtol=1e-12,
+                                   atol=1e-12 * np.abs(d[f"smax{i}"]).max())
+    f = S.fatigue_life_field(d["fat_s1"], d["fat_s2"], 48e6)
+    for k, v in f.items():
+        np.testing.assert_allclose(v, d["fat_" + k], rtol=1e-13)
+    assert S.sn_alt_stress_at(1e6) == float(d["sn_alt_1e6"])

@@ -578,6 +578,33 @@ int tof_eig_sens(tof_ctx* ctx, const double* qK, const double* qM, double lam, d
   return TOF_OK;
 }
 
+int tof_stress(tof_ctx* ctx, const double* B_c, const double* D, int dtype, const void* u, int nvec,
+               const double* rho, double* sigma, double* vm, double* smax, void* stream) {
+  if (!ctx || !B_c || !D || !u || nvec < 1 || (dtype != TOF_F32 && dtype != TOF_F64)) return TOF_ERR_ARG;
+  Ctx& c = ctx->c;
+  if (launch_stress(c, B_c, D, dtype == TOF_F64, u, nvec, rho, sigma, vm, smax, (cudaStream_t)stream)) {
+    c.last_error = "tof_stress: launch failed";
+    return TOF_ERR_CUDA;
+  }
+  return TOF_OK;
+}
+
+int tof_stress_invariants(long long n, const double* sigma, double* vm, double* smax, void* stream) {
+  if (n < 0 || (n > 0 && !sigma)) return TOF_ERR_ARG;
+  return launch_stress_invariants(n, sigma, vm, smax, (cudaStream_t)stream) ? TOF_ERR_CUDA : TOF_OK;
+}
+
+int tof_fatigue(long long n, const double* s1, const double* s2, double sigma_uts, double s_design_pa, double* out,
+                void* stream) {
+  if (n < 0 || (n > 0 && (!s1 || !s2 || !out)) || !(sigma_uts > 0.0)) return TOF_ERR_ARG;
+  return launch_fatigue(n, s1, s2, sigma_uts, s_design_pa, out, (cudaStream_t)stream) ? TOF_ERR_CUDA : TOF_OK;
+}
+
+int tof_sn_life(long long n, const double* sigma_eq, double* life, void* stream) {
+  if (n < 0 || (n > 0 && (!sigma_eq || !life))) return TOF_ERR_ARG;
+  return launch_sn_life(n, sigma_eq, life, (cudaStream_t)stream) ? TOF_ERR_CUDA : TOF_OK;
+}
+
 int tof_effective_mass(tof_ctx* ctx, const double* modes, int nmodes, int direction, double* out, void* stream) {
   if (!ctx || !modes || !out || nmodes < 1 || nmodes > 8 || direction < 0 || direction > 2) return TOF_ERR_ARG;
   Ctx& c = ctx->c;

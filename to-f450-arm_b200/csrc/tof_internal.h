@@ -115,6 +115,14 @@ void launch_convert(const void* src, bool src64, void* dst, bool dst64, long lon
 void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s);
 void launch_add_f32_to_f64(long long n, const float* d, double* x, cudaStream_t s);
 
+// stress and fatigue (tof_stress.cu)
+int launch_stress(Ctx& c, const double* B, const double* D, bool f64, const void* u, int nvec, const double* rho,
+                  double* sigma, double* vm, double* smax, cudaStream_t s);
+int launch_stress_invariants(long long n, const double* sigma, double* vm, double* smax, cudaStream_t s);
+int launch_fatigue(long long n, const double* s1, const double* s2, double uts, double s_design_pa, double* out,
+                   cudaStream_t s);
+int launch_sn_life(long long n, const double* sigma_eq, double* life, cudaStream_t s);
+
 // PCG (tof_pcg.cu)
 int pcg_plain64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int* iters, double* relres,
                 int* status, cudaStream_t s);

@@ -66,6 +66,10 @@ SIGNATURES = {
     "tof_compliance_sens": (c_int, [P, c_int, P, P, P, P, P]),
     "tof_eig_sens": (c_int, [P, P, P, c_double, c_double, P, P]),
     "tof_effective_mass": (c_int, [P, P, c_int, c_int, POINTER(c_double), P]),
+    "tof_stress": (c_int, [P, POINTER(c_double), POINTER(c_double), c_int, P, c_int, P, P, P, P, P]),
+    "tof_stress_invariants": (c_int, [c_longlong, P, P, P, P]),
+    "tof_fatigue": (c_int, [c_longlong, P, P, c_double, c_double, P, P]),
+    "tof_sn_life": (c_int, [c_longlong, P, P, P]),
     "tof_filter_create": (c_int, [c_int, c_int, c_int, POINTER(c_double), c_int, c_int, c_int, POINTER(c_uint8),
                                   POINTER(c_uint8), POINTER(P)]),
     "tof_filter_apply": (c_int, [P, c_int, P, P, P]),

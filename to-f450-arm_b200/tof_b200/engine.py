@@ -207,6 +207,25 @@ class DesignContext:
         L.check("tof_mg_apply", self.lib.tof_mg_apply(self.h, L.ptr(r4), L.ptr(e), r4.shape[0], _stream()), self.h)
         return e
 
+    def stress(self, u4: torch.Tensor, B_c: np.ndarray, D: np.ndarray, rho_grid: torch.Tensor = None,
+               sigma=True, vm=True, smax=True):
+        """Element-centre stress of R node4 displacement vectors over the full
+        grid: (sigma (R, NE, 6), vm (R, NE), smax (R, NE)), each None unless
+        requested.  rho_grid None: the density set by set_density."""
+        u4 = u4.contiguous()
+        R = u4.shape[0]
+        dev = self.device
+        o_s = torch.empty((R, self.NE, 6), dtype=torch.float64, device=dev) if sigma else None
+        o_v = torch.empty((R, self.NE), dtype=torch.float64, device=dev) if vm else None
+        o_m = torch.empty((R, self.NE), dtype=torch.float64, device=dev) if smax else None
+        rho = None if rho_grid is None else rho_grid.to(dev, torch.float64).contiguous()
+        Bc = np.ascontiguousarray(B_c, np.float64)
+        Dm = np.ascontiguousarray(D, np.float64)
+        L.check("tof_stress", self.lib.tof_stress(self.h, L.dptr(Bc), L.dptr(Dm),
+                                                  L.F64 if u4.dtype == torch.float64 else L.F32, L.ptr(u4), R,
+                                                  L.ptr(rho), L.ptr(o_s), L.ptr(o_v), L.ptr(o_m), _stream()), self.h)
+        return o_s, o_v, o_m
+
     def effective_mass(self, modes4: torch.Tensor, direction=2) -> np.ndarray:
         m = modes4.to(torch.float64).contiguous()
         out = (c_double * m.shape[0])()
@@ -248,6 +267,18 @@ class DensityFilter:
                 self.h = None
         except Exception:
             pass
+
+
+def stress_invariants(sigma: torch.Tensor):
+    """(von Mises, largest principal stress) of (..., 6) Voigt stresses on the
+    device (src/fem.py:582-602)."""
+    lib = L.load()
+    s = sigma.to(torch.float64).contiguous()
+    n = s.numel() // 6
+    vm = torch.empty(s.shape[:-1], dtype=torch.float64, device=s.device)
+    smax = torch.empty_like(vm)
+    L.check("tof_stress_invariants", lib.tof_stress_invariants(n, L.ptr(s), L.ptr(vm), L.ptr(smax), _stream()))
+    return vm, smax
 
 
 def oc_update(x: torch.Tensor, dc: torch.Tensor, V_e: float, target_volume: float, move: float) -> torch.Tensor:

@@ -296,6 +296,39 @@ class FEM3D:
         ce = ctx.quadform(L.OP_K, u4)[0]
         return ce[torch.as_tensor(self.active_ids, device=ctx.device)].cpu().numpy()
 
+    def compute_stress(self, u, rho_active):
+        """Voigt stress (n_active, 6) at the element centres,
+        rho_e D B_c u_e (src/fem.py:564-579)."""
+        sig, _, _ = self.stress_fields(u, rho_active, vm=False, smax=False)
+        return sig
+
+    def stress_fields(self, u, rho_active, sigma=True, vm=True, smax=True):
+        """(sigma (n_active, 6), von Mises (n_active,), largest principal
+        (n_active,)) in one kernel pass; u may be one (N,) vector or (R, N)."""
+        ctx = self.device()
+        U = np.asarray(u, dtype=np.float64)
+        one = U.ndim == 1
+        u4 = ctx.pack(torch.from_numpy(U))
+        rho = self.rho_to_grid(rho_active)
+        s, v, m = ctx.stress(u4, self.B_centre, self.D_solid, rho, sigma=sigma, vm=vm, smax=smax)
+        ids = torch.as_tensor(self.active_ids, device=ctx.device)
+        pick = (lambda t: None if t is None else (t[0, ids] if one else t[:, ids]).cpu().numpy())
+        return pick(s), pick(v), pick(m)
+
+    def von_mises(self, stress):
+        """von Mises equivalent of (..., 6) Voigt stresses (src/fem.py:582-589)."""
+        return self._invariants(stress)[0]
+
+    def principal_stress_max(self, stress):
+        """Largest principal stress per row (src/fem.py:592-602)."""
+        return self._invariants(stress)[1]
+
+    def _invariants(self, stress):
+        from .engine import stress_invariants
+        dev = self.device().device
+        vm, sm = stress_invariants(torch.as_tensor(np.asarray(stress, dtype=np.float64), device=dev))
+        return vm.cpu().numpy(), sm.cpu().numpy()
+
     def total_mass(self, rho_active):
         """src/fem.py:618-621."""
         g = self.geom
