@@ -227,6 +227,14 @@ int tof_fatigue(long long n, const double* s1, const double* s2, double sigma_ut
  * from the PA12 S-N curve (sn_life, src/fatigue.py:24-65). */
 int tof_sn_life(long long n, const double* sigma_eq, double* life, void* stream);
 
+/* Modal-superposition FRF magnitude at ndof DOFs and npts frequencies:
+ * out[d][i] = |sum_k V[d][k]^2 / ((w_k^2 - w_i^2) + 2 i zeta w_k w_i)|,
+ * w = 2 pi f (modal_frf_at_dof, src/plotting.py:378-399).  V: device FP64
+ * [ndof][m] mode-shape values at the DOFs, fk_hz: device [m] natural
+ * frequencies, f_hz: device [npts]; out: device FP64 [ndof][npts]. */
+int tof_modal_frf(long long ndof, int m, const double* V, const double* fk_hz, long long npts, const double* f_hz,
+                  double zeta, double* out, void* stream);
+
 /* Density filter on an nx*ny*nz element grid (x fastest) with a (kx,ky,kz)
  * weight array (z slowest: w[(qz*ky + qy)*kx + qx], odd sizes) and a mask
  * (NE bytes).  Replaces topopt.cone_kernel / filter_field

@@ -32,3 +32,17 @@ def first_excitable(freqs, eff, thresh=EXCITABLE_FRAC):
         if e >= thresh:
             return float(f), float(e), k
     return None, None, None
+
+
+def modal_frf_at_dof(frequencies_Hz, mode_shapes, dof_idx, freq_range_Hz=(10.0, 1500.0), n_pts=600,
+                     modal_damping=0.02):
+    """|H_dd(f)| = |sum_k v_k[d]^2 / ((w_k^2 - w^2) + 2 i zeta w_k w)| on a
+    geometric frequency grid (src/plotting.py:378-399)."""
+    f = np.geomspace(freq_range_Hz[0], freq_range_Hz[1], n_pts)
+    w = 2.0 * np.pi * f
+    wk = 2.0 * np.pi * np.asarray(frequencies_Hz)
+    v = np.asarray(mode_shapes)[dof_idx, :]
+    H = np.zeros(n_pts, dtype=complex)
+    for k in range(len(wk)):
+        H += v[k] ** 2 / (wk[k] ** 2 - w ** 2 + 2j * modal_damping * wk[k] * w)
+    return f, np.abs(H)

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference source tree (read-only):
 
-    python tests/golden/make_golden.py --ref /root/reference [--skip-arm] [--only stress]
+    python tests/golden/make_golden.py --ref /root/reference [--skip-arm] [--only stress|frf]
 
 The reference (NinhGhoster/TO-F450-arm, pure Python + SciPy) is imported from
 its own `src/` and `sims/` packages and driven with the synthetic geometries of
@@ -257,6 +257,41 @@ def make_stress(rfem):
     return out
 
 
+def make_frf(rfem):
+    """Modal-superposition FRF |H_dd(f)| (src/plotting.py:378-399) of the tiny
+    domain's modes at three DOFs.  src/plotting.py imports matplotlib at module
+    level; only `modal_frf_at_dof` (pure NumPy) is used, so matplotlib is
+    stubbed for the import when it is absent."""
+    import types
+    if "matplotlib" not in sys.modules:
+        try:
+            import matplotlib  # noqa: F401
+        except ImportError:
+            mpl = types.ModuleType("matplotlib")
+            mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+            mpl.pyplot.rcParams = {}            # module-level style settings only
+            mpl.colors = types.ModuleType("matplotlib.colors")
+            for n in ("LogNorm", "Normalize", "BoundaryNorm"):
+                setattr(mpl.colors, n, object)
+            sys.modules.update({"matplotlib": mpl, "matplotlib.pyplot": mpl.pyplot,
+                                "matplotlib.colors": mpl.colors})
+    from src import plotting as rplot
+    g = tiny_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    rho = np.random.default_rng(1).uniform(0.03, 1.0, fem.n_active)
+    freqs, modes, lam = fem.modal_analysis(rho, n_modes=4, tip_mass_kg=0.06)
+    tip = g.motor_mount_top_nodes()
+    dofs = np.array([3 * tip[0] + 2, 3 * tip[-1] + 1, fem.free_dofs[7]])
+    out = dict(freqs=freqs, modes=modes, dofs=dofs)
+    for i, d in enumerate(dofs):
+        f, H = rplot.modal_frf_at_dof(freqs, modes, int(d))
+        out[f"f{i}"], out[f"H{i}"] = f, H
+    f, H = rplot.modal_frf_at_dof(freqs, modes, int(dofs[0]), freq_range_Hz=(50.0, 4000.0), n_pts=257,
+                                  modal_damping=0.05)
+    out["f_alt"], out["H_alt"] = f, H
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -267,11 +302,15 @@ def main():
     if a.only == "stress":
         np.savez_compressed(os.path.join(HERE, "stress.npz"), **make_stress(rfem))
         return
+    if a.only == "frf":
+        np.savez_compressed(os.path.join(HERE, "frf.npz"), **make_frf(rfem))
+        return
     np.savez_compressed(os.path.join(HERE, "tiny.npz"), **make_tiny(rfem, rtop, rmp))
     np.savez_compressed(os.path.join(HERE, "oc.npz"), **make_oc(rtop))
     np.savez_compressed(os.path.join(HERE, "simp_small.npz"), **make_simp(rfem, rtop))
     np.savez_compressed(os.path.join(HERE, "cantilever.npz"), **make_cantilever(rfem, rmp))
     np.savez_compressed(os.path.join(HERE, "stress.npz"), **make_stress(rfem))
+    np.savez_compressed(os.path.join(HERE, "frf.npz"), **make_frf(rfem))
     if not a.skip_arm:
         np.savez_compressed(os.path.join(HERE, "arm.npz"), **make_arm(rfem, rmp))
 

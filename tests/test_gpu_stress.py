@@ -74,3 +74,19 @@ def test_arm_stress_matches_oracle():
         _close(sig[k], ref, 1e-12)
         _close(vm[k], S.von_mises(ref), 1e-12)
         _close(sm[k], S.principal_stress_max(ref), 1e-10)
+
+
+def test_modal_frf_matches_reference(golden):
+    """Modal-superposition FRF (src/plotting.py:378-399) on the device against
+    the reference's own output, one DOF at a time and batched over DOFs."""
+    from tof_b200.modal import modal_frf, modal_frf_at_dof
+    d = golden("frf")
+    for i, dof in enumerate(d["dofs"]):
+        f, H = modal_frf_at_dof(d["freqs"], d["modes"], int(dof))
+        np.testing.assert_array_equal(f, d[f"f{i}"])
+        np.testing.assert_allclose(H, d[f"H{i}"], rtol=1e-12)
+    f, H = modal_frf_at_dof(d["freqs"], d["modes"], int(d["dofs"][0]), (50.0, 4000.0), 257, 0.05)
+    np.testing.assert_allclose(H, d["H_alt"], rtol=1e-12)
+    Hb = modal_frf(d["freqs"], d["modes"][d["dofs"], :], d["f0"]).cpu().numpy()
+    for i in range(3):
+        np.testing.assert_allclose(Hb[i], d[f"H{i}"], rtol=1e-12)

@@ -170,3 +170,14 @@ def test_oracle_stress_and_fatigue(golden):
     for k, v in f.items():
         np.testing.assert_allclose(v, d["fat_" + k], rtol=1e-13)
     assert S.sn_alt_stress_at(1e6) == float(d["sn_alt_1e6"])
+
+
+def test_oracle_frf(golden):
+    from oracle.modal import modal_frf_at_dof
+    d = golden("frf")
+    for i, dof in enumerate(d["dofs"]):
+        f, H = modal_frf_at_dof(d["freqs"], d["modes"], int(dof))
+        np.testing.assert_array_equal(f, d[f"f{i}"])
+        np.testing.assert_allclose(H, d[f"H{i}"], rtol=1e-13)
+    f, H = modal_frf_at_dof(d["freqs"], d["modes"], int(d["dofs"][0]), (50.0, 4000.0), 257, 0.05)
+    np.testing.assert_allclose(H, d["H_alt"], rtol=1e-13)

@@ -605,6 +605,12 @@ int tof_sn_life(long long n, const double* sigma_eq, double* life, void* stream)
   return launch_sn_life(n, sigma_eq, life, (cudaStream_t)stream) ? TOF_ERR_CUDA : TOF_OK;
 }
 
+int tof_modal_frf(long long ndof, int m, const double* V, const double* fk_hz, long long npts, const double* f_hz,
+                  double zeta, double* out, void* stream) {
+  if (ndof < 0 || npts < 0 || m < 1 || (ndof * npts > 0 && (!V || !fk_hz || !f_hz || !out))) return TOF_ERR_ARG;
+  return launch_modal_frf(ndof, m, V, fk_hz, npts, f_hz, zeta, out, (cudaStream_t)stream) ? TOF_ERR_CUDA : TOF_OK;
+}
+
 int tof_effective_mass(tof_ctx* ctx, const double* modes, int nmodes, int direction, double* out, void* stream) {
   if (!ctx || !modes || !out || nmodes < 1 || nmodes > 8 || direction < 0 || direction > 2) return TOF_ERR_ARG;
   Ctx& c = ctx->c;

@@ -123,6 +123,10 @@ int launch_fatigue(long long n, const double* s1, const double* s2, double uts, 
                    cudaStream_t s);
 int launch_sn_life(long long n, const double* sigma_eq, double* life, cudaStream_t s);
 
+// modal FRF (tof_frf.cu)
+int launch_modal_frf(long long ndof, int m, const double* V, const double* fk_hz, long long npts, const double* f_hz,
+                     double zeta, double* out, cudaStream_t s);
+
 // PCG (tof_pcg.cu)
 int pcg_plain64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int* iters, double* relres,
                 int* status, cudaStream_t s);

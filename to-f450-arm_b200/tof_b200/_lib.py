@@ -70,6 +70,7 @@ SIGNATURES = {
     "tof_stress_invariants": (c_int, [c_longlong, P, P, P, P]),
     "tof_fatigue": (c_int, [c_longlong, P, P, c_double, c_double, P, P]),
     "tof_sn_life": (c_int, [c_longlong, P, P, P]),
+    "tof_modal_frf": (c_int, [c_longlong, c_int, P, P, c_longlong, P, c_double, P, P]),
     "tof_filter_create": (c_int, [c_int, c_int, c_int, POINTER(c_double), c_int, c_int, c_int, POINTER(c_uint8),
                                   POINTER(c_uint8), POINTER(P)]),
     "tof_filter_apply": (c_int, [P, c_int, P, P, P]),
