@@ -69,8 +69,8 @@ bool encode_node4_map(CUtensorMap* m, const void* base, const Grid& g, int R, bo
 
 static int pow2ceil(int r) { return r <= 1 ? 1 : r <= 2 ? 2 : r <= 4 ? 4 : 8; }
 
-long long& launch_counter() {
-  static long long n = 0;
+std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> n{0};
   return n;
 }
 bool& capturing() {
@@ -129,7 +129,7 @@ extern "C" {
 
 int tof_version(void) { return 100; }
 
-long long tof_launch_count(void) { return launch_counter(); }
+long long tof_launch_count(void) { return launch_counter().load(); }
 
 const char* tof_last_error(const tof_ctx* ctx) {
   return ctx ? ctx->c.last_error.c_str() : g_create_error.c_str();
@@ -158,6 +158,23 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
     c.sp.mass_threshold = simp->mass_threshold; c.sp.mass_q = simp->mass_q;
   }
   c.max_rhs = pow2ceil(std::max(max_rhs, max_modes));
+  // the largest per-CTA shared memory any kernel of this context asks for:
+  // the FP64 persistent PCG tile (two halo blocks of max_rhs vectors)
+  {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t nfe = size_t(TX + 1) * (TY + 1) * (TZ + 1);
+    size_t need = 2 * size_t(halo_bytes<double>(c.g, c.max_rhs)) + sizeof(double) * (kKeBlocksLen + nfe);
+    need = ((need + 15) & ~size_t(15)) + sizeof(double) * 3 * c.max_rhs * 32 + 16;
+    if (optin > 0 && need > size_t(optin)) {
+      g_create_error = "tof_ctx_create: tile " + std::to_string(TX) + "x" + std::to_string(TY) + "x" +
+                       std::to_string(TZ) + " needs " + std::to_string(need) + " B of shared memory per block with " +
+                       std::to_string(c.max_rhs) + " vectors (limit " + std::to_string(optin) + " B)";
+      delete h_;
+      return TOF_ERR_ARG;
+    }
+  }
   c.max_modes = max_modes;
   const Grid& g = c.g;
   auto fail = [&](const std::string& m) {

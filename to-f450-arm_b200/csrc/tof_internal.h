@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -14,10 +15,13 @@ namespace tof {
 
 // Host-side count of kernels this library launched (graph replays add their
 // node count; launches recorded into a graph being captured are not counted).
-long long& launch_counter();
-bool& capturing();
+// process-wide count of kernels launched (atomic: contexts may be driven
+// from several host threads); launches recorded into a graph capture are
+// counted when the graph is replayed instead
+std::atomic<long long>& launch_counter();
+bool& capturing();   // per host thread
 inline void count_launch(long long n = 1) {
-  if (!capturing()) launch_counter() += n;
+  if (!capturing()) launch_counter().fetch_add(n, std::memory_order_relaxed);
 }
 // Error message of calls without a context (returned by tof_last_error(NULL)).
 void set_global_error(const std::string& msg);

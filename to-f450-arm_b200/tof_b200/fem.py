@@ -117,6 +117,9 @@ class FEM3D:
                self.MASS_THRESHOLD, self.MASS_PENALTY_Q)
         if self._ctx is None or key != self._ctx_key:
             g = self.geom
+            if self.tile == "auto":                       # measured once per grid (tof_b200.autotune)
+                from .autotune import tune_tile
+                self.tile = tune_tile(self)
             self._ctx = DesignContext(g.nx, g.ny, g.nz, (g.dx, g.dy, g.dz), self.Ke_solid, self.Me_solid,
                                       active_grid=self.in_arm, fixed_dofs=self.fixed_dofs,
                                       simp=(self.SIMP_PENALTY, self.E_MIN_FRAC, self.MASS_THRESHOLD,

@@ -46,3 +46,22 @@ def arm_hollow_analysis(mode="mixed", tile=None):
     geom = C.arm_geometry()
     fem = FEM3D(geom, C.PA12, mode=mode, tile=tile)
     return geom, fem, C.arm_hollow_density(geom), C.arm_static_loads(geom)[0]
+
+
+SWEEP_VFS = (0.08, 0.10, 0.20, 0.30, 0.50)
+
+
+def sweep_designs(vfs=SWEEP_VFS, fine=True, n_modes=8, tile="auto"):
+    """The uneven design sweep: arm designs on the 2 mm grid (110 x 14 x 12)
+    at the given volume fractions, plus (fine=True) one design on the 1 mm
+    grid (220 x 28 x 24, ~480k DOF) at vf 0.08; each with the four load cases
+    and the n_modes lowest modes.  Returns [(name, geom, fem, opt)] for
+    tof_b200.batch.DesignSweep."""
+    out = []
+    for vf in vfs:
+        geom, fem, opt = arm_simp(mode="mixed", vf=vf, n_modes=n_modes, tile=tile)
+        out.append((f"2mm_vf{vf:.2f}", geom, fem, opt))
+    if fine:
+        geom, fem, opt = arm_simp(mode="mixed", nx=220, ny=28, nz=24, h=1e-3, vf=0.08, n_modes=n_modes, tile=tile)
+        out.append(("1mm_vf0.08", geom, fem, opt))
+    return out
