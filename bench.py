@@ -222,6 +222,31 @@ def solver_comparison(torch, L, C):
     return out
 
 
+def design_sweep_extra(torch, steps=2):
+    """The uneven design sweep (five 2 mm arm designs at vf 0.08-0.50 and one
+    1 mm design, 4 load cases and 8 modes each): design iterations per second
+    with the designs advanced concurrently (one stream and host thread each)
+    and one after another, from the same start, after one warm-up iteration."""
+    from tof_b200.batch import DesignSweep
+    from tof_b200.workloads import sweep_designs
+    res = {}
+    for mode in ("concurrent", "sequential"):
+        designs = sweep_designs()
+        sw = DesignSweep(designs)
+        sw.step(concurrent=(mode == "concurrent"))
+        t = sum(sw.step(concurrent=(mode == "concurrent")) for _ in range(steps))
+        res[mode] = len(designs) * steps / t
+        if mode == "concurrent":
+            res["designs"] = [dict(name=n, grid=[g.nx, g.ny, g.nz], dofs=int(g.n_dofs), tile=list(f.device().tile))
+                              for n, g, f, _ in designs]
+        for _, _, f, _ in designs:
+            f.device().close()
+    res.update(unit="design iter/s", steps=steps,
+               speedup_concurrent=res["concurrent"] / res["sequential"],
+               timing="wall clock between device synchronisations around each sweep iteration")
+    return res
+
+
 def reduce_max(x: float, torch, device) -> float:
     """Max of a per-rank scalar over all ranks (a replica job is as fast as
     its slowest rank); the value itself on a single process."""
@@ -346,6 +371,7 @@ def own_arm(a, rank, world, local_rank):
         line["speedup_mixed_vs_fp64"] = value / (1.0 / t64)
         fem64.device().close()
         line["solvers_hollow_arm"] = solver_comparison(torch, L, C)
+        line["design_sweep"] = design_sweep_extra(torch)
         # the reference algorithm on the host cores (bounded sample)
         from oracle.cpu_bench import simp_iteration_sample
         rho = C.arm_hollow_density(geom)

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference source tree (read-only):
 
-    python tests/golden/make_golden.py --ref /root/reference [--skip-arm] [--only stress|frf]
+    python tests/golden/make_golden.py --ref /root/reference [--skip-arm] [--only stress|frf|arm3d|arm3d_modes]
 
 The reference (NinhGhoster/TO-F450-arm, pure Python + SciPy) is imported from
 its own `src/` and `sims/` packages and driven with the synthetic geometries of
@@ -292,6 +292,31 @@ def make_frf(rfem):
     return out
 
 
+def make_arm3d(with_modes=False):
+    """The reference's production domain (src/mesh3d.py ArmGeometry3D):
+    masks, clamped nodes, tip-mass nodes and load vectors; with_modes: the
+    lowest 6 exact FP64 frequencies of the solid domain with the 60 g tip
+    mass (src/fem.py:400-470 with the exact eigensolver)."""
+    from src.mesh3d import ArmGeometry3D
+    g = ArmGeometry3D()
+    m = g.build_masks()
+    out = {k: v for k, v in m.items()}
+    out["fixed_nodes"] = g.fixed_nodes()
+    out["motor_nodes"] = g.motor_mount_top_nodes()
+    for tag, F in (("thrust", (0.0, 0.0, -15.0)), ("inplane", (3.0, -4.0, 2.0))):
+        d, v = g.load_dofs_for_force(F)
+        out[f"{tag}_dofs"], out[f"{tag}_vals"] = d, v
+    d, v = g.load_dofs_for_moment_Mz(0.3)
+    out["mz_dofs"], out["mz_vals"] = d, v
+    if with_modes:
+        import src.fem as rfem
+        fem = rfem.FEM3D(g, mat_ref(rfem))
+        t0 = time.time()
+        freqs, modes, lam = fem.modal_analysis(np.ones(fem.n_active), n_modes=6, tip_mass_kg=0.06)
+        out = dict(freqs=freqs, lam=lam, n_free=len(fem.free_dofs), seconds=time.time() - t0)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -302,6 +327,12 @@ def main():
     if a.only == "stress":
         np.savez_compressed(os.path.join(HERE, "stress.npz"), **make_stress(rfem))
         return
+    if a.only == "arm3d":
+        np.savez_compressed(os.path.join(HERE, "arm3d.npz"), **make_arm3d())
+        return
+    if a.only == "arm3d_modes":
+        np.savez_compressed(os.path.join(HERE, "arm3d_modes.npz"), **make_arm3d(with_modes=True))
+        return
     if a.only == "frf":
         np.savez_compressed(os.path.join(HERE, "frf.npz"), **make_frf(rfem))
         return
@@ -311,7 +342,9 @@ def main():
     np.savez_compressed(os.path.join(HERE, "cantilever.npz"), **make_cantilever(rfem, rmp))
     np.savez_compressed(os.path.join(HERE, "stress.npz"), **make_stress(rfem))
     np.savez_compressed(os.path.join(HERE, "frf.npz"), **make_frf(rfem))
+    np.savez_compressed(os.path.join(HERE, "arm3d.npz"), **make_arm3d())
     if not a.skip_arm:
+        np.savez_compressed(os.path.join(HERE, "arm3d_modes.npz"), **make_arm3d(with_modes=True))
         np.savez_compressed(os.path.join(HERE, "arm.npz"), **make_arm(rfem, rmp))
 
 
