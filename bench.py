@@ -367,7 +367,10 @@ def own_arm(a, rank, world, local_rank):
         opt64.step()
         torch.cuda.synchronize()
         t64, _ = time_steps(opt64.step, 1, flush, torch)
-        line["fp64_plain"] = {"iter_s": 1.0 / t64, "ms_per_step": t64 * 1e3, "steps": 1}
+        h64 = opt64.history
+        line["fp64_plain"] = {"iter_s": 1.0 / t64, "ms_per_step": t64 * 1e3, "steps": 1,
+                              "modal_converged": bool(h64["modal_converged"][-1]),
+                              "modal_iters": int(h64["modal_iters"][-1]), "pcg_iters": int(h64["pcg_iters"][-1])}
         line["speedup_mixed_vs_fp64"] = value / (1.0 / t64)
         fem64.device().close()
         line["solvers_hollow_arm"] = solver_comparison(torch, L, C)

@@ -19,6 +19,8 @@
 // convergence is accepted; a final FP64 Rayleigh-Ritz on fresh products gives
 // the returned pairs.
 #include <math.h>
+
+#include <algorithm>
 #include <stdio.h>
 
 #include "tof_internal.h"
@@ -33,11 +35,15 @@ constexpr int kMaxBasis = 24;
 constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M products
 // Below its rounding floor (~eps * lambda_max / lambda_1 of the pencil) the
 // iteration stops converging and its basis can degrade.  The best iterate
-// (smallest worst wanted residual) is kept aside; the iteration stops, not
-// converged, when the residual grows kLobDiverge-fold over that best or has
-// not improved for kLobStall iterations, and the best iterate is returned.
+// (smallest worst wanted residual) is kept aside.  Once that best is below
+// kLobNearFloor (far from the plateaus near 1 that a Jacobi-preconditioned
+// start goes through) the iteration stops, not converged, when the residual
+// grows kLobDiverge-fold over the best or has not improved for
+// max(kLobStall, iterations taken to reach the best), and the best iterate
+// is returned.
 constexpr int kLobStall = 500;
 constexpr double kLobDiverge = 1e3;
+constexpr double kLobNearFloor = 1e-3;
 
 // ---------------------------------------------------------------------------
 // residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, written to
@@ -606,7 +612,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       it_best = it;
       for (int j = 0; j < nmodes; ++j) best_res[j] = rres[j];
       cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
-    } else if (worst > kLobDiverge * best || it - it_best >= kLobStall) {
+    } else if (best < kLobNearFloor &&
+               (worst > kLobDiverge * best || it - it_best >= std::max(kLobStall, it_best))) {
       use_best = true;
       break;
     }
