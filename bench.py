@@ -304,7 +304,12 @@ def own_arm(a, rank, world, local_rank):
                               "steps": a.steps, "warmup": a.warmup, "ms_per_step": total / a.steps * 1e3,
                               "gpu_launches": int(launches), "profiling_run": True}), flush=True)
         return
-    # ---- end to end through the public API with host buffers
+    # ---- end to end through the public API with host buffers, over the same
+    # design iterations as the device-timed run (reset, same warm-up)
+    opt.reset()
+    for _ in range(a.warmup):
+        opt.step()
+    torch.cuda.synchronize()
     n_design = int(opt.design_ids.numel())
     x_host = torch.empty(n_design, dtype=torch.float64, pin_memory=True)
     x_host.copy_(opt.x[opt.design_ids].cpu())
@@ -320,7 +325,7 @@ def own_arm(a, rank, world, local_rank):
         torch.cuda.current_stream().synchronize()
         x_host.copy_(out_host)
 
-    n_e2e = max(1, min(a.steps, 5))
+    n_e2e = a.steps
     e2e_total, _ = time_steps(e2e_step, n_e2e, flush, torch)
     e2e_total = reduce_max(e2e_total, torch, "cuda")
     e2e = {"value": replica_value(world, n_e2e, e2e_total), "unit": "iter/s",
