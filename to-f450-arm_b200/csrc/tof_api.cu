@@ -255,7 +255,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.lw32, 18 * MM * V));
   A(dalloc(c, &c.lw64, 21 * MM * V));
   A(dalloc(c, &c.gram, 8 * 576));
-  A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 576));
+  A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 1152));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
   if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error);
   A(cudaMemcpy(c.Ke64, Ke, 576 * 8, cudaMemcpyHostToDevice));

@@ -111,6 +111,9 @@ void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb,
 struct ColMap {
   int col[24];
 };
+// G1 = A[:, cols]^T B1[:, cols], G2 = A[:, cols]^T B2[:, cols] (n x n) in one pass
+void launch_gram2_cols(Ctx& c, bool f64, const void* A, const void* B1, const void* B2, const ColMap& cols, int n,
+                       double* G1, double* G2, cudaStream_t s);
 // G = A[:, ma]^T B[:, mb] (na x nb), same kernels as launch_gram
 void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na, const void* B, const ColMap& mb,
                       int nb, double* G, cudaStream_t s);

@@ -377,6 +377,115 @@ __global__ void __launch_bounds__(256) k_gram_reduce(int nblocks, int npair, con
   if (lane == 0) G[p] = s;
 }
 
+// Two Gram matrices with a shared left block, G1 = S^T B1 and G2 = S^T B2
+// (the K and M Grams of LOBPCG's Rayleigh-Ritz), from one staging of S: the
+// same warp tiling as k_gram_partial with 16-node chunks (three staged
+// blocks), partials [block][2][576].
+constexpr int kGram2Chunk = 16;
+constexpr int kGram2Ld = 4 * kGram2Chunk + 2;      // 66 doubles: rows 4 banks apart
+
+template <typename T>
+__global__ void __launch_bounds__(kGramThreads) k_gram2_partial(int NN, const T* __restrict__ A,
+                                                               const T* __restrict__ B1, const T* __restrict__ B2,
+                                                               ColMap cols, int n, long long vstride, double* part) {
+  using V4 = typename Vec4<T>::type;
+  __shared__ __align__(16) double sm[72 * kGram2Ld];   // rows 0..23: S, 24..47: B1, 48..71: B2
+  static_assert(72 * kGram2Ld >= 8 * 576, "reduction scratch");
+  for (int i = threadIdx.x; i < 72 * kGram2Ld; i += blockDim.x) sm[i] = 0.0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rg = lane & 7, cg = lane >> 3;
+  double acc1[3][6], acc2[3][6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) acc1[i][j] = acc2[i][j] = 0.0;
+  const int nchunks = (NN + kGram2Chunk - 1) / kGram2Chunk;
+  const int nstage = 3 * n * kGram2Chunk;
+  for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int n0 = ch * kGram2Chunk;
+    const int cnt = min(kGram2Chunk, NN - n0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nstage; idx += blockDim.x) {
+      const int v = idx / kGram2Chunk, q = idx % kGram2Chunk;
+      if (q >= cnt) continue;
+      const int blk = v / n, col = v % n;
+      const T* base = blk == 0 ? A : blk == 1 ? B1 : B2;
+      const V4 x = reinterpret_cast<const V4*>(base + cols.col[col] * vstride)[n0 + q];
+      double* d = sm + (blk * 24 + col) * kGram2Ld + 4 * q;
+      reinterpret_cast<double2*>(d)[0] = make_double2(double(x.x), double(x.y));
+      reinterpret_cast<double2*>(d)[1] = make_double2(double(x.z), 0.0);
+    }
+    __syncthreads();
+    const double* pa = sm + 3 * rg * kGram2Ld;
+    const double* pb1 = sm + (24 + 6 * cg) * kGram2Ld;
+    const double* pb2 = sm + (48 + 6 * cg) * kGram2Ld;
+    for (int q = w; q < cnt; q += kGramThreads / 32) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int o = 4 * q + c;
+        double a[3], b1[6], b2[6];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) a[i] = pa[i * kGram2Ld + o];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) { b1[j] = pb1[j * kGram2Ld + o]; b2[j] = pb2[j * kGram2Ld + o]; }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 6; ++j) {
+            acc1[i][j] = fma(a[i], b1[j], acc1[i][j]);
+            acc2[i][j] = fma(a[i], b2[j], acc2[i][j]);
+          }
+      }
+    }
+  }
+  double* red = sm;                                    // [warp][576], one Gram at a time
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) red[w * 576 + (3 * rg + i) * 24 + 6 * cg + j] = g == 0 ? acc1[i][j] : acc2[i][j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, col = e % n;
+      double sum = 0.0;
+#pragma unroll
+      for (int k = 0; k < kGramThreads / 32; ++k) sum += red[k * 576 + r * 24 + col];
+      part[(size_t)blockIdx.x * 1152 + g * 576 + e] = sum;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_gram2_reduce(int nblocks, int npair, const double* __restrict__ part,
+                                                      double* G1, double* G2) {
+  const int p = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (p >= 2 * npair) return;
+  const int g = p / npair, e = p % npair;
+  double s = 0.0;
+  for (int b = lane; b < nblocks; b += 32) s += part[(size_t)b * 1152 + g * 576 + e];
+  s = warp_sum(s);
+  if (lane == 0) (g == 0 ? G1 : G2)[e] = s;
+}
+
+void launch_gram2_cols(Ctx& c, bool f64, const void* A, const void* B1, const void* B2, const ColMap& cols, int n,
+                       double* G1, double* G2, cudaStream_t s) {
+  const int nchunks = ceil_div(c.g.NN, kGram2Chunk);
+  int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
+  if (blocks < 1) blocks = 1;
+  const long long vs = (long long)c.g.NN * 4;
+  if (f64)
+    k_gram2_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, (const double*)B1,
+                                                           (const double*)B2, cols, n, vs, c.gram_part);
+  else
+    k_gram2_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, (const float*)B1,
+                                                          (const float*)B2, cols, n, vs, c.gram_part);
+  count_launch();
+  k_gram2_reduce<<<ceil_div(2 * n * n, 8), 256, 0, s>>>(blocks, n * n, c.gram_part, G1, G2);
+  count_launch();
+}
+
 void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na, const void* B, const ColMap& mb,
                       int nb, double* G, cudaStream_t s) {
   const int nchunks = ceil_div(c.g.NN, kGramChunk);

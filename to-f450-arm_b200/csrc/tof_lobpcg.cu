@@ -396,51 +396,61 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
 // ---------------------------------------------------------------------------
 // block update: Xn = S C, Pn = S[:, nb:] C[nb:, :] for S, KS, MS
 // ---------------------------------------------------------------------------
-// One thread per (node, block in {S, KS, MS}, component): ncols inputs, 2 nb
-// outputs, all in registers.  The 4th (padding) component of the outputs is
-// never written and stays zero.
+// One thread per (node, block in {S, KS, MS}): the ncols input node records
+// stream in as whole (coalesced) 4-component loads; the 2 nb outputs
+// accumulate in registers and are stored with a zero 4th component.
 template <typename T>
 __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, ColMap cols, long long vs,
                                                     const T* __restrict__ S, const T* __restrict__ KS,
                                                     const T* __restrict__ MS, const double* __restrict__ C,
                                                     T* S2, T* KS2, T* MS2) {
+  using V4 = typename Vec4<T>::type;
   __shared__ T sC[kMaxBasis * 8];
   for (int i = threadIdx.x; i < ncols * nb; i += blockDim.x) sC[i] = T(C[i]);
   __syncthreads();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= 9LL * NN) return;
+  if (t >= 3LL * NN) return;
   const int n = int(t % NN);
-  const int bc = int(t / NN);
-  const int b = bc / 3, c = bc % 3;
+  const int b = int(t / NN);
   const T* src = b == 0 ? S : b == 1 ? KS : MS;
   T* dst = b == 0 ? S2 : b == 1 ? KS2 : MS2;
-  const size_t o = 4 * (size_t)n + c;
-  T in[kMaxBasis];
+  T x[8][3], p[8][3];
 #pragma unroll
-  for (int j = 0; j < kMaxBasis; ++j) in[j] = j < ncols ? src[cols.col[j] * vs + o] : T(0);
+  for (int k = 0; k < 8; ++k)
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    if (k >= nb) break;
-    T x = T(0), p = T(0);
+    for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = T(0);
 #pragma unroll
-    for (int j = 0; j < kMaxBasis; ++j) {
-      if (j < ncols) {
-        const T cf = sC[j * nb + k];
-        x = fma(cf, in[j], x);
-        if (j >= nb) p = fma(cf, in[j], p);
+  for (int j = 0; j < kMaxBasis; ++j) {
+    if (j < ncols) {
+      const V4 v = reinterpret_cast<const V4*>(src + cols.col[j] * vs)[n];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        if (k < nb) {
+          const T cf = sC[j * nb + k];
+          x[k][0] = fma(cf, v.x, x[k][0]); x[k][1] = fma(cf, v.y, x[k][1]); x[k][2] = fma(cf, v.z, x[k][2]);
+          if (j >= nb) {
+            p[k][0] = fma(cf, v.x, p[k][0]); p[k][1] = fma(cf, v.y, p[k][1]); p[k][2] = fma(cf, v.z, p[k][2]);
+          }
+        }
       }
     }
-    dst[k * vs + o] = x;
-    dst[(2 * nb + k) * vs + o] = p;
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (k < nb) {
+      V4 o, q;
+      o.x = x[k][0]; o.y = x[k][1]; o.z = x[k][2]; o.w = T(0);
+      q.x = p[k][0]; q.y = p[k][1]; q.z = p[k][2]; q.w = T(0);
+      reinterpret_cast<V4*>(dst + k * vs)[n] = o;
+      reinterpret_cast<V4*>(dst + (2 * nb + k) * vs)[n] = q;
+    }
   }
 }
 
-// X' = S[:, cols] C (first nb vectors of the destination), P' = the part of
-// that product from the columns after the first nb (vectors 2 nb .. 3 nb - 1)
 template <typename T>
 static void launch_lob_update(int NN, int nb, int ncols, const ColMap& cols, long long vs, const T* S, const T* KS,
                               const T* MS, const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s) {
-  k_lob_update<T><<<int((9LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2);
+  k_lob_update<T><<<int((3LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2);
   count_launch();
 }
 
@@ -510,8 +520,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
   if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
   // initial Rayleigh-Ritz on X alone
-  launch_gram(c, f64, B.S[cur], nb, B.KS[cur], nb, GK, s);
-  launch_gram(c, f64, B.S[cur], nb, B.MS[cur], nb, GM, s);
+  launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], identity_cols(), nb, GK, GM, s);
   lob_small_eig(c, nb, nb, drop, s);
   const ColMap ident = identity_cols();
   launch_lob_update<T>(NN, nb, nb, ident, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
@@ -655,8 +664,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (it > 0)
       for (int k = 0; k < na; ++k) cols.col[ncols++] = 2 * nb + act[k];
     for (int k = ncols; k < 24; ++k) cols.col[k] = 0;
-    launch_gram_cols(c, f64, B.S[cur], cols, ncols, B.KS[cur], cols, ncols, GK, s);
-    launch_gram_cols(c, f64, B.S[cur], cols, ncols, B.MS[cur], cols, ncols, GM, s);
+    launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s);
     lob_small_eig(c, ncols, nb, drop, s);
     cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
     launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
@@ -674,8 +682,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (!use_best) cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
   if (launch_matvec(c, 0, true, X6, KX6, nb, nullptr, s)) return -2;
   if (launch_matvec(c, 1, true, X6, MX6, nb, nullptr, s)) return -2;
-  launch_gram(c, true, X6, nb, KX6, nb, GK, s);
-  launch_gram(c, true, X6, nb, MX6, nb, GM, s);
+  launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, GK, GM, s);
   lob_small_eig(c, nb, nb, 1e-14, s);
   // X64 = X6 C (first nmodes columns)
   {
