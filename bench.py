@@ -222,6 +222,42 @@ def solver_comparison(torch, L, C):
     return out
 
 
+def production_domain_extra(torch):
+    """The reference's production domain (ArmGeometry3D, 198k free DOF, solid,
+    60 g tip mass): seconds per static solve (thrust + motor torque, true
+    relative residual 1e-8) in both forms and per 6-mode modal solve
+    (relative residual 1e-8) in the mixed form, after a warm-up solve."""
+    from tof_b200 import configs as C
+    from tof_b200.fem import FEM3D
+    from tof_b200.geometry3d import ArmGeometry3D
+    g = ArmGeometry3D()
+    F = g.load_vector(F=(0.0, 0.0, -15.0), Mz=0.3)
+    out = {"grid": [g.nx, g.ny, g.nz]}
+    for mode in ("mixed", "fp64"):
+        fem = FEM3D(g, C.PA12, mode=mode)
+        rho = np.ones(fem.n_active)
+        fem.SOLVE_RTOL = 1e-8
+        fem.solve(rho, F)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u = fem.solve(rho, F)
+        torch.cuda.synchronize()
+        out[f"static_s_{mode}"] = time.perf_counter() - t0
+        out[f"compliance_{mode}"] = float(F @ u)
+        if mode == "mixed":
+            out["free_dofs"] = int(len(fem.free_dofs))
+            fem.modal_analysis(rho, n_modes=6, tip_mass_kg=C.TIP_MASS_KG, tol=1e-8)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            freqs, _, _ = fem.modal_analysis(rho, n_modes=6, tip_mass_kg=C.TIP_MASS_KG, tol=1e-8)
+            torch.cuda.synchronize()
+            out["modal_s_mixed"] = time.perf_counter() - t0
+            out["freqs_Hz"] = [float(f) for f in freqs]
+        fem.device().close()
+    out["timing"] = "wall clock between device synchronisations, one solve each after a warm-up solve"
+    return out
+
+
 def design_sweep_extra(torch, steps=2):
     """The uneven design sweep (five 2 mm arm designs at vf 0.08-0.50 and one
     1 mm design, 4 load cases and 8 modes each): design iterations per second
@@ -380,6 +416,7 @@ def own_arm(a, rank, world, local_rank):
         fem64.device().close()
         line["solvers_hollow_arm"] = solver_comparison(torch, L, C)
         line["design_sweep"] = design_sweep_extra(torch)
+        line["production_domain"] = production_domain_extra(torch)
         # the reference algorithm on the host cores (bounded sample)
         from oracle.cpu_bench import simp_iteration_sample
         rho = C.arm_hollow_density(geom)
