@@ -10,10 +10,10 @@
 //                                        or one FP32 multigrid V-cycle)
 //   KW, MW                              (matrix-free block matvecs)
 //   G_K = S^T K S, G_M = S^T M S        (S = [X W_act P_act], FP64 Gram)
-//   Rayleigh-Ritz on (G_K, G_M)         (k_small_eig: one warp; Cholesky of
+//   Rayleigh-Ritz on (G_K, G_M)         (k_small_eig: one CTA; Cholesky of
 //                                        the scaled G_M, or SVQB when the
-//                                        basis is ill-conditioned; implicit
-//                                        symmetric QR for the small problem)
+//                                        basis is ill-conditioned; parallel
+//                                        cyclic Jacobi for the small problem)
 //   X, P, KX, MX, KP, MP <- S C         (k_lob_update)
 // K X, M X, K P, M P are recomputed every kLobRefresh iterations and before
 // convergence is accepted; a final FP64 Rayleigh-Ritz on fresh products gives
@@ -87,174 +87,183 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
 }
 
 // ---------------------------------------------------------------------------
-// Symmetric eigensolver for n <= 24, one warp, matrix in shared memory:
-// Householder tridiagonalisation (Golub & Van Loan, Matrix Computations,
-// 4th ed., Alg. 8.3.1) with the reflections accumulated into Q, then the
-// implicit symmetric QR step with Wilkinson shift (Alg. 8.3.2) inside the
-// deflation loop of Alg. 8.3.3.  Lane i owns row i of A and Q.  The warp
-// tests the off-diagonals for deflation in parallel (ballot); lane 0 chases
-// the bulge on the (d, e) diagonals with rsqrt-based Givens rotations and
-// records them; the warp then applies the recorded rotations to the rows of
-// Q.  Backward stable: eigenvalue errors ~ eps ||A||.
-// On return d[k] / Q[:, k] are the eigenpairs (unsorted); false if the QR
-// iteration did not converge within its sweep budget.
+// Symmetric eigensolver for K <= 24, one CTA, matrix in shared memory:
+// cyclic two-sided Jacobi (Golub & Van Loan, Matrix Computations, 4th ed.,
+// Alg. 8.5.2 / 8.5.3) with the parallel round-robin ordering (ibid.,
+// Sec. 8.5.5): the NP / 2 disjoint index pairs of a round (NP = K rounded up
+// to even; a pair holding the padding index is the identity) are rotated at
+// once: NP / 2 threads compute the rotations, then thread (i, j) writes
+// element (i, j) of J^T A J and of V J to the other buffer.  A pair (p, q) is rotated unless
+// a_pq^2 <= tol^2 |a_pp a_qq| -- the relative criterion, which gives the
+// small eigenvalues of a positive definite matrix to high relative accuracy
+// (Demmel & Veselic, SIAM J. Matrix Anal. Appl. 13 (1992)) -- or
+// |a_pq| <= kJacAbs ||A||_F, the rounding level of the rotations themselves
+// (the backward error of QR), which ends the iteration on the nearly
+// singular Gram matrices of the SVQB path.  The iteration ends at the first
+// round whose input matrix meets the criterion everywhere.  The four terms
+// of an element are summed as (t1 + (t2 + t3)) + t4 with t2, t3 exchanged
+// under i <-> j, so the matrix stays exactly symmetric.  The critical path
+// is one rotation, one element update and two barriers per round (~1 400
+// cycles measured on a B200, a dependent chain of shared loads and FP64
+// operations): 6-10 sweeps of K - 1 rounds on the graded Rayleigh-Ritz
+// matrices of LOBPCG, against one Givens rotation per step of the serial QR
+// bulge chase on one warp.
+// On return d[k] / V[:, k] are the eigenpairs (unsorted); false if
+// kJacSweeps sweeps did not converge.  A is destroyed; A2 and V2 are scratch.
 // ---------------------------------------------------------------------------
 constexpr int LDA = kMaxBasis + 1;
-constexpr int kEigThreads = 32;
-constexpr int kQrSweeps = 30 * kMaxBasis;
+constexpr int kEigThreads = kMaxBasis * kMaxBasis;   // one thread per element
+constexpr int kJacSweeps = 40;
+constexpr double kJacTol = 1e-14;
+constexpr double kJacAbs = 1e-15;
 
-struct EigScratch {
-  double e[kMaxBasis], rc[kMaxBasis], rs[kMaxBasis], v[kMaxBasis], w[kMaxBasis];
-};
+__device__ __forceinline__ bool jac_offdiag_live(double apq, double app, double aqq, double floor2) {
+  const double a2 = apq * apq;
+  return a2 > kJacTol * kJacTol * fabs(app * aqq) && a2 > floor2;
+}
 
-__device__ bool warp_syev(double (*A)[LDA], double (*Q)[LDA], double* d, EigScratch& S, int n) {
-  const int lane = threadIdx.x;
-  const unsigned full = 0xffffffffu;
-  double* e = S.e;
-  double* v = S.v;
-  double* w = S.w;
-  for (int j = 0; j < n; ++j)
-    if (lane < n) Q[lane][j] = (lane == j) ? 1.0 : 0.0;
-  __syncwarp();
-  // --- tridiagonalisation: A <- H_k A H_k, Q <- Q H_k
-  for (int k = 0; k + 2 < n; ++k) {
-    const int i = lane;
-    const bool below = i > k && i < n;
-    const double xi = below ? A[i][k] : 0.0;
-    const double sig = warp_sum((i > k + 1 && i < n) ? xi * xi : 0.0);
-    const double alpha = __shfl_sync(full, xi, k + 1);
-    if (!(sig > 0.0)) {                    // column already reduced
-      __syncwarp();
-      continue;
-    }
-    const double mu = sqrt(alpha * alpha + sig);
-    const double v1 = alpha <= 0.0 ? alpha - mu : -sig / (alpha + mu);
-    const double beta = 2.0 * v1 * v1 / (sig + v1 * v1);
-    if (below) v[i] = (i == k + 1) ? 1.0 : xi / v1;
-    __syncwarp();
-    // p = beta A' v, w = p - (beta / 2)(p^T v) v
-    double p = 0.0;
-    if (below)
-      for (int j = k + 1; j < n; ++j) p = fma(A[i][j], v[j], p);
-    p *= beta;
-    const double pv = warp_sum(below ? p * v[i] : 0.0);
-    if (below) w[i] = p - 0.5 * beta * pv * v[i];
-    double sq = 0.0;                       // (Q v)_i
-    if (i < n)
-      for (int j = k + 1; j < n; ++j) sq = fma(Q[i][j], v[j], sq);
-    __syncwarp();
-    if (below)
-      for (int j = k + 1; j < n; ++j) A[i][j] -= v[i] * w[j] + w[i] * v[j];
-    if (i < n)
-      for (int j = k + 1; j < n; ++j) Q[i][j] -= beta * sq * v[j];
-    if (i == k + 1) { A[k + 1][k] = mu; A[k][k + 1] = mu; }
-    if (i > k + 1 && i < n) { A[i][k] = 0.0; A[k][i] = 0.0; }
-    __syncwarp();
+__device__ bool cta_jacobi(double (*A)[LDA], double (*A2)[LDA], double (*V)[LDA], double (*V2)[LDA], double* d,
+                           int K) {
+  // per index x of the round: the new row x of J^T A is
+  // jal[x] A[x, :] + jbe[x] A[jmt[x], :] (the same for the columns of A J)
+  __shared__ double jal[kMaxBasis + 1], jbe[kMaxBasis + 1];
+  __shared__ int jmt[kMaxBasis + 1];
+  __shared__ unsigned char jpq[kMaxBasis - 1][kMaxBasis / 2][2];   // the round-robin schedule
+  __shared__ double red[kEigThreads / 32];
+  __shared__ double fro2;
+  const int t = threadIdx.x;
+  const int i = t / kMaxBasis, j = t % kMaxBasis;
+  const bool own = i < K && j < K;
+  const int NP = K + (K & 1), M = NP - 1;
+  if (t < M * (NP / 2)) {
+    // pair k of round r on NP = M + 1 players (M odd): player 0 meets
+    // circle position r, positions r + k and r - k meet each other
+    const int r = t / (NP / 2), k = t % (NP / 2);
+    int p = k == 0 ? 0 : (r + k) % M + 1;
+    int q = k == 0 ? r + 1 : (r - k + M) % M + 1;
+    jpq[r][k][0] = (unsigned char)min(p, q);
+    jpq[r][k][1] = (unsigned char)max(p, q);
   }
-  if (lane < n) d[lane] = A[lane][lane];
-  if (lane + 1 < n) e[lane] = A[lane + 1][lane];
-  __syncwarp();
-  // --- implicit symmetric QR on (d, e)
-  const double eps = 2.220446049250313e-16;
-  for (int sweep = 0; sweep < kQrSweeps; ++sweep) {
-    bool live = false;
-    if (lane + 1 < n) {
-      if (fabs(e[lane]) <= eps * (fabs(d[lane]) + fabs(d[lane + 1]))) e[lane] = 0.0;
-      else live = true;
-    }
-    const unsigned bits = __ballot_sync(full, live);
-    __syncwarp();
-    if (bits == 0u) return true;
-    const int top = 31 - __clz(bits);      // last nonzero off-diagonal
-    const int hi = top + 1;
-    const unsigned zeros = ~bits & ((1u << top) - 1u);
-    const int lo = zeros ? 32 - __clz(zeros) : 0;
-    if (lane == 0) {
-      // Wilkinson shift from the trailing 2 x 2 of the block
-      const double dl = 0.5 * (d[hi - 1] - d[hi]);
-      const double eh = e[hi - 1];
-      const double sg = dl >= 0.0 ? 1.0 : -1.0;
-      const double mu = d[hi] - eh * eh / (dl + sg * sqrt(dl * dl + eh * eh));
-      double x = d[lo] - mu, z = e[lo], bulge = 0.0;
-      double dk = d[lo], ek = e[lo];
-      for (int k = lo; k < hi; ++k) {
-        if (k > lo) { x = e[k - 1]; z = bulge; }
-        const double r2 = x * x + z * z;
-        double c = 1.0, sn = 0.0, r = 0.0;
-        if (r2 > 0.0) {
-          const double ir = rsqrt(r2);
-          c = x * ir; sn = z * ir; r = r2 * ir;
-        }
-        if (k > lo) e[k - 1] = r;
-        const double dd = d[k + 1];
-        const double a = dk, b = ek;
-        const double cc = c * c, ss = sn * sn, cs = c * sn;
-        d[k] = cc * a + 2.0 * cs * b + ss * dd;
-        dk = ss * a - 2.0 * cs * b + cc * dd;   // new d[k + 1]
-        e[k] = cs * (dd - a) + (cc - ss) * b;
-        d[k + 1] = dk;
-        if (k + 1 < hi) {
-          const double en = e[k + 1];
-          bulge = sn * en;
-          ek = c * en;
-          e[k + 1] = ek;
-        }
-        S.rc[k] = c; S.rs[k] = sn;
-      }
-    }
-    __syncwarp();
-    if (lane < n) {
-      for (int k = lo; k < hi; ++k) {       // Q <- Q G_k
-        const double c = S.rc[k], sn = S.rs[k];
-        const double qa = Q[lane][k], qb = Q[lane][k + 1];
-        Q[lane][k] = c * qa + sn * qb;
-        Q[lane][k + 1] = -sn * qa + c * qb;
-      }
-    }
-    __syncwarp();
+  const double a2 = warp_sum(own ? A[i][j] * A[i][j] : 0.0);   // ||A||_F^2
+  if ((t & 31) == 0) red[t >> 5] = a2;
+  if (own) V[i][j] = (i == j) ? 1.0 : 0.0;
+  __syncthreads();
+  if (t == 0) {
+    double f = 0.0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) f += red[w];
+    fro2 = f;
   }
-  return false;
+  __syncthreads();
+  const double floor2 = kJacAbs * kJacAbs * fro2;
+  double(*Ac)[LDA] = A;
+  double(*An)[LDA] = A2;
+  double(*Vc)[LDA] = V;
+  double(*Vn)[LDA] = V2;
+  bool conv = M <= 0;
+  for (int it = 0, r = 0; !conv && it < kJacSweeps * M; ++it, r = (r + 1 == M) ? 0 : r + 1) {
+    if (t < NP / 2) {
+      const int p = jpq[r][t][0], q = jpq[r][t][1];
+      double c = 1.0, sn = 0.0;
+      bool rot = false;
+      if (q < K) {
+        const double app = Ac[p][p], aqq = Ac[q][q], apq = Ac[p][q];
+        if (jac_offdiag_live(apq, app, aqq, floor2)) {
+          // tan(2 phi) = 2 a_pq / (a_qq - a_pp), |phi| <= pi / 4:
+          // c = (r + |d|) / sqrt(2 r (r + |d|)), s = sgn(d) e / sqrt(2 r (r + |d|))
+          const double dd = aqq - app, e = 2.0 * apq;
+          const double r2 = fma(dd, dd, e * e);
+          const double rr = r2 * rsqrt(r2);
+          const double ad = fabs(dd);
+          const double iw = rsqrt(2.0 * rr * (rr + ad));
+          c = (rr + ad) * iw;
+          sn = (dd >= 0.0 ? e : -e) * iw;
+          rot = true;
+        }
+      }
+      jal[p] = c; jbe[p] = -sn; jmt[p] = rot ? q : p;
+      jal[q] = c; jbe[q] = sn;  jmt[q] = rot ? p : q;
+    }
+    __syncthreads();
+    bool bad = false;
+    if (own) {
+      const double ai = jal[i], bi = jbe[i], aj = jal[j], bj = jbe[j];
+      const int mi = jmt[i], mj = jmt[j];
+      const double aij = Ac[i][j];
+      bad = i != j && jac_offdiag_live(aij, Ac[i][i], Ac[j][j], floor2);
+      double v;
+      if (mi == j && mi != i) {
+        v = 0.0;                           // the rotated pair's off-diagonal
+      } else {
+        const double t1 = (ai * aj) * aij;
+        const double t2 = (ai * bj) * Ac[i][mj];
+        const double t3 = (bi * aj) * Ac[mi][j];
+        const double t4 = (bi * bj) * Ac[mi][mj];
+        v = (t1 + (t2 + t3)) + t4;
+      }
+      An[i][j] = v;
+      Vn[i][j] = fma(bj, Vc[i][mj], aj * Vc[i][j]);
+    }
+    // the round's input already met the criterion: nothing was rotated
+    conv = !__syncthreads_or(bad);
+    if (!conv) {
+      double(*tA)[LDA] = Ac; Ac = An; An = tA;
+      double(*tV)[LDA] = Vc; Vc = Vn; Vn = tV;
+    }
+  }
+  if (own && i == j) d[i] = Ac[i][i];
+  if (Vc != V && own) V[i][j] = Vc[i][j];
+  __syncthreads();
+  return conv;
 }
 
 // In-place Cholesky B = L L^T of a symmetric n x n matrix (lower triangle
 // and diagonal become L); idiag[k] = 1 / L[k][k].  false (uniformly across
-// the warp) when a pivot is not above piv_min: the basis is too close to
-// dependent for Cholesky-based orthonormalisation.  Lane i keeps row i in
-// registers; column k is broadcast with shuffles.
-__device__ bool warp_chol(double (*B)[LDA], double* idiag, int n, double piv_min) {
-  const int lane = threadIdx.x;
-  const unsigned full = 0xffffffffu;
-  constexpr int NB = kMaxBasis;
-  double b[NB];
-#pragma unroll
-  for (int j = 0; j < NB; ++j) b[j] = (lane < n && j < n) ? B[lane][j] : 0.0;
-  bool ok = true;
-#pragma unroll
-  for (int k = 0; k < NB; ++k) {
-    if (k < n && ok) {
-      const double pk = __shfl_sync(full, b[k], k);
-      if (!(pk > piv_min)) {
-        ok = false;
-      } else {
-        const double ir = rsqrt(pk);
-        if (lane == k) { b[k] = pk * ir; if (lane < NB) idiag[k] = ir; }
-        else if (lane > k) b[k] *= ir;
-        const double lik = b[k];
-#pragma unroll
-        for (int j = k + 1; j < NB; ++j) {
-          const double ljk = __shfl_sync(full, b[k], j);
-          if (lane > k && j <= lane && j < n) b[j] = fma(-lik, ljk, b[j]);
-        }
-      }
-    }
+// the CTA) when a pivot is not above piv_min: the basis is too close to
+// dependent for Cholesky-based orthonormalisation.  Right-looking, one
+// barrier per column: at step k each thread (i, j), k < j <= i, applies
+// B[i][j] -= B[i][k] B[j][k] / d_k with column k and the pivot d_k already
+// final; the columns are scaled by d_k^-1/2 at the end.  Loops, not
+// unrolled code: each step runs once, so straight-line code would be bound
+// by instruction fetch.
+// (The CTA has one thread per element of a kMaxBasis x kMaxBasis matrix:
+// thread t owns (t / kMaxBasis, t % kMaxBasis), a compile-time divisor.)
+__device__ bool cta_chol(double (*B)[LDA], double* idiag, int n, double piv_min) {
+  const int t = threadIdx.x, i = t / kMaxBasis, j = t % kMaxBasis;
+  for (int k = 0; k < n; ++k) {
+    const double pk = B[k][k];
+    if (!(pk > piv_min)) return false;               // the same value in every thread
+    const double rp = rsqrt(pk);
+    if (k < j && j <= i && i < n) B[i][j] = fma(-B[i][k] * (rp * rp), B[j][k], B[i][j]);
+    __syncthreads();
   }
-  if (ok && lane < n) {
-#pragma unroll
-    for (int j = 0; j < NB; ++j)
-      if (j <= lane && j < n) B[lane][j] = b[j];
+  if (t < n) idiag[t] = rsqrt(B[t][t]);
+  __syncthreads();
+  if (j <= i && i < n) B[i][j] *= idiag[j];
+  __syncthreads();
+  return true;
+}
+
+// T <- L^-1 T (forward substitution, n x nc), L the lower triangle of B and
+// idiag = 1 / diag(L); one barrier per row.
+__device__ void cta_forward(double (*T)[LDA], double (*B)[LDA], const double* idiag, int n, int nc) {
+  const int t = threadIdx.x, i = t / kMaxBasis, j = t % kMaxBasis;
+  for (int l = 0; l + 1 < n; ++l) {
+    if (i > l && i < n && j < nc) T[i][j] = fma(-B[i][l] * idiag[l], T[l][j], T[i][j]);
+    __syncthreads();
   }
-  __syncwarp();
-  return ok;
+  if (i < n && j < nc) T[i][j] *= idiag[i];
+  __syncthreads();
+}
+
+// T <- L^-T T (backward substitution, n x nc); one barrier per row.
+__device__ void cta_backward(double (*T)[LDA], double (*B)[LDA], const double* idiag, int n, int nc) {
+  const int t = threadIdx.x, i = t / kMaxBasis, j = t % kMaxBasis;
+  for (int l = n - 1; l > 0; --l) {
+    if (i < l && j < nc) T[i][j] = fma(-B[l][i] * idiag[l], T[l][j], T[i][j]);
+    __syncthreads();
+  }
+  if (i < n && j < nc) T[i][j] *= idiag[i];
+  __syncthreads();
 }
 
 // Rayleigh-Ritz: the m smallest eigenpairs of G_K c = theta G_M c (n x n).
@@ -264,7 +273,7 @@ __device__ bool warp_chol(double (*B)[LDA], double* idiag, int n, double piv_min
 // (Stathopoulos & Wu, SIAM J. Sci. Comput. 23 (2002)): D G_M D is
 // eigendecomposed, directions with eigenvalue below drop_tol * max are
 // discarded, and the standard problem is solved in the remaining
-// M-orthonormal basis.
+// M-orthonormal basis.  One CTA, one thread per matrix element.
 // Outputs: C (n x m, row-major), theta (m), info[0] = kept rank (or -1).
 constexpr double kCholPivot = 1e-8;
 
@@ -272,56 +281,43 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
                                                           const double* __restrict__ GM, double drop_tol, double* C,
                                                           double* theta, int* info) {
   __shared__ double A[kMaxBasis][LDA], B[kMaxBasis][LDA], V[kMaxBasis][LDA], Z[kMaxBasis][LDA];
+  __shared__ double A2[kMaxBasis][LDA], V2[kMaxBasis][LDA];
   __shared__ double D[kMaxBasis], ev[kMaxBasis], idg[kMaxBasis];
-  __shared__ EigScratch S;
   __shared__ int keep[kMaxBasis], order[kMaxBasis];
   __shared__ int kr;
-  const int lane = threadIdx.x;
-  if (lane < n) {
-    const double b = GM[lane * n + lane];
-    D[lane] = b > 0.0 ? 1.0 / sqrt(b) : 0.0;
+  const int tid = threadIdx.x;
+  if (tid < n) {
+    const double b = GM[tid * n + tid];
+    D[tid] = b > 0.0 ? rsqrt(b) : 0.0;
   }
-  __syncwarp();
-  for (int w = lane; w < n * n; w += 32) {
+  __syncthreads();
+  for (int w = tid; w < n * n; w += blockDim.x) {
     const int i = w / n, j = w % n;
     A[i][j] = 0.5 * (GK[i * n + j] + GK[j * n + i]) * D[i] * D[j];
     B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
   }
-  __syncwarp();
+  __syncthreads();
+  const bool chol = cta_chol(B, idg, n, kCholPivot);
   bool ok = true;
   int K = n;
-  const bool chol = warp_chol(B, idg, n, kCholPivot);
   if (chol) {
-    // V = L^-1 A (lane j: column j), then Z = V L^-T (lane j: row j of Z)
-    if (lane < n) {
-      for (int i = 0; i < n; ++i) {
-        double t = A[i][lane];
-        for (int l = 0; l < i; ++l) t = fma(-B[i][l], V[l][lane], t);
-        V[i][lane] = t * idg[i];
-      }
-    }
-    __syncwarp();
-    if (lane < n) {
-      for (int i = 0; i < n; ++i) {
-        double t = V[lane][i];
-        for (int l = 0; l < i; ++l) t = fma(-B[i][l], Z[lane][l], t);
-        Z[lane][i] = t * idg[i];
-      }
-    }
-    __syncwarp();
-    for (int w = lane; w < n * n; w += 32) {
-      const int a = w / n, b = w % n;
-      A[a][b] = 0.5 * (Z[a][b] + Z[b][a]);
-    }
-    __syncwarp();
+    // A <- L^-1 A, then Z <- L^-1 A^T = (L^-1 A_0 L^-T)^T, symmetrised into A
+    const int ti = tid / kMaxBasis, tj = tid % kMaxBasis;
+    const bool te = ti < n && tj < n;
+    cta_forward(A, B, idg, n, n);
+    if (te) Z[tj][ti] = A[ti][tj];
+    __syncthreads();
+    cta_forward(Z, B, idg, n, n);
+    if (te) A[ti][tj] = 0.5 * (Z[ti][tj] + Z[tj][ti]);
+    __syncthreads();
   } else {
-    for (int w = lane; w < n * n; w += 32) {             // B was overwritten by the failed Cholesky
+    for (int w = tid; w < n * n; w += blockDim.x) {       // B was overwritten by the failed Cholesky
       const int i = w / n, j = w % n;
       B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
     }
-    __syncwarp();
-    ok = warp_syev(B, V, ev, S, n);
-    if (lane == 0) {
+    __syncthreads();
+    ok = cta_jacobi(B, A2, V, V2, ev, n);
+    if (tid == 0) {
       double bmax = 0.0;
       for (int i = 0; i < n; ++i) bmax = fmax(bmax, ev[i]);
       int k = 0;
@@ -329,61 +325,55 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
         if (ev[i] > drop_tol * bmax) keep[k++] = i;
       kr = k;
     }
-    __syncwarp();
+    __syncthreads();
     K = kr;
-    for (int w = lane; w < n * K; w += 32) {              // Z = V[:, keep] / sqrt(lambda)
+    for (int w = tid; w < n * K; w += blockDim.x) {        // Z = V[:, keep] / sqrt(lambda)
       const int i = w / K, a = w % K;
       Z[i][a] = V[i][keep[a]] / sqrt(ev[keep[a]]);
     }
-    __syncwarp();
-    for (int w = lane; w < n * K; w += 32) {              // V <- A Z
+    __syncthreads();
+    for (int w = tid; w < n * K; w += blockDim.x) {        // V <- A Z
       const int i = w / K, a = w % K;
       double s = 0.0;
       for (int j = 0; j < n; ++j) s = fma(A[i][j], Z[j][a], s);
       V[i][a] = s;
     }
-    __syncwarp();
-    for (int w = lane; w < K * K; w += 32) {              // B <- Z^T V
+    __syncthreads();
+    for (int w = tid; w < K * K; w += blockDim.x) {        // B <- Z^T V
       const int a = w / K, b = w % K;
       double s = 0.0;
       for (int j = 0; j < n; ++j) s = fma(Z[j][a], V[j][b], s);
       B[a][b] = s;
     }
-    __syncwarp();
-    for (int w = lane; w < K * K; w += 32) {
+    __syncthreads();
+    for (int w = tid; w < K * K; w += blockDim.x) {
       const int a = w / K, b = w % K;
       A[a][b] = 0.5 * (B[a][b] + B[b][a]);
     }
-    __syncwarp();
+    __syncthreads();
   }
-  ok = warp_syev(A, V, ev, S, K) && ok;
-  if (lane == 0) {
-    for (int i = 0; i < K; ++i) order[i] = i;
-    for (int i = 0; i < K; ++i)
-      for (int j = i + 1; j < K; ++j)
-        if (ev[order[j]] < ev[order[i]]) { const int t = order[i]; order[i] = order[j]; order[j] = t; }
-    info[0] = (K >= m && ok) ? K : -1;
+  ok = cta_jacobi(A, A2, V, V2, ev, K) && ok;
+  if (tid < K) {                                           // ascending order (ties by index)
+    const double e = ev[tid];
+    int rank = 0;
+    for (int j = 0; j < K; ++j) rank += (ev[j] < e || (ev[j] == e && j < tid)) ? 1 : 0;
+    order[rank] = tid;
   }
-  __syncwarp();
+  if (tid == 0) info[0] = (K >= m && ok) ? K : -1;
+  __syncthreads();
   if (K < m || !ok) return;
-  if (lane < m) theta[lane] = ev[order[lane]];
+  if (tid < m) theta[tid] = ev[order[tid]];
   if (chol) {
-    // C[:, k] = D L^-T U[:, order[k]]: lane k back-substitutes its column
-    if (lane < m) {
-      const int o = order[lane];
-      for (int i = n - 1; i >= 0; --i) {
-        double t = V[i][o];
-        for (int l = i + 1; l < n; ++l) t = fma(-B[l][i], Z[l][lane], t);
-        Z[i][lane] = t * idg[i];
-      }
-    }
-    __syncwarp();
-    for (int w = lane; w < n * m; w += 32) {
+    // C = D L^-T U[:, order[:m]]
+    for (int w = tid; w < n * m; w += blockDim.x) Z[w / m][w % m] = V[w / m][order[w % m]];
+    __syncthreads();
+    cta_backward(Z, B, idg, n, m);
+    for (int w = tid; w < n * m; w += blockDim.x) {
       const int i = w / m, k = w % m;
       C[i * m + k] = D[i] * Z[i][k];
     }
   } else {
-    for (int w = lane; w < n * m; w += 32) {              // C = D Z U[:, order[:m]]
+    for (int w = tid; w < n * m; w += blockDim.x) {        // C = D Z U[:, order[:m]]
       const int i = w / m, k = w % m;
       double s = 0.0;
       for (int a = 0; a < K; ++a) s = fma(Z[i][a], V[a][order[k]], s);
