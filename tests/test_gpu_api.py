@@ -86,12 +86,15 @@ def test_simp_matches_reference_run(golden):
 def test_mixed_simp_iterations_match_oracle():
     """The mixed (multigrid, batched) form of the benchmark iteration (4 load
     cases incl. the inertial load, 6 modes, 500 Hz target, seeded start
-    design) against the oracle's exact-solve iteration on a small arm."""
+    design) against the oracle's exact-solve iteration on a small arm.  The
+    modal tolerance sits one decade above the FP64 LOBPCG residual floor on
+    SIMP designs (~1e-7); a residual of 1e-6 bounds the frequency error far
+    below the 1e-8 checked here."""
     from oracle.fem import OracleFEM
     from oracle.topopt import OracleSIMP
     from tof_b200 import configs as C
     from tof_b200.workloads import arm_simp
-    geom, fem, opt = arm_simp(mode="mixed", nx=24, ny=6, nz=6, modal_tol=1e-7)
+    geom, fem, opt = arm_simp(mode="mixed", nx=24, ny=6, nz=6, modal_tol=1e-6)
     ofem = OracleFEM(geom, C.PA12.E, C.PA12.nu, C.PA12.rho)
     x0 = C.arm_design_start(geom).astype(float)
     ref = OracleSIMP(geom, ofem, opt.F_list, vol_frac=0.08, r_min_mm=3.0, min_freq_Hz=500.0, tip_mass_kg=0.06,

@@ -15,9 +15,13 @@
 //   K_E = sum_children P_c^T (D_c f_c Ke D_c) P_c using the Kronecker
 //   structure P_c = W_c (x) I3 (8 x 8 scalar weights), so no matrix is
 //   assembled; levels >= 1 store one dense 24x24 FP32 matrix per element;
-// * smoother: damped Jacobi, nu pre- and nu post-sweeps (a symmetric V-cycle,
-//   hence an SPD preconditioner for CG); the fine-level sweeps use the
-//   TMA-tiled matrix-free stencil;
+// * smoother: Chebyshev polynomial in D^-1 A of degree nu on the interval
+//   [lambda / 30, 1.3 lambda] (lambda a power-iteration estimate of
+//   lambda_max(D^-1 A) per level), as the same three-term recurrence before
+//   and after the coarse correction (a symmetric V-cycle, hence an SPD
+//   preconditioner for CG); damped Jacobi with the same number of sweeps
+//   when TOF_MG_SMOOTHER=jacobi.  The fine-level sweeps use the TMA-tiled
+//   matrix-free stencil;
 // * coarsest level: dense FP64 inverse, built by one CTA (Cholesky, then
 //   L^-T L^-1), applied as a dense matvec.
 #include <math.h>
@@ -39,6 +43,16 @@ constexpr int kMaxLevels = 10;
 // omega * lambda_max near 1.6, inside the stable range (0, 2).
 constexpr float kOmegaScale = 1.3333f;
 constexpr int kPowerIters = 10;
+// Chebyshev smoothing interval [lambda / kChebRatio, kChebUpper lambda]: the
+// upper end must cover the power iteration's underestimate of lambda_max
+// (2-9 % on the SIMP arm levels), since above the interval the polynomial
+// amplifies the error and the V-cycle stops being positive definite; the
+// ratio and margin were chosen on the SIMP arm designs (a CPU model of this
+// V-cycle: 14 % fewer MG-PCG iterations than damped Jacobi at equal sweeps).
+constexpr float kChebUpper = 1.3f;
+constexpr float kChebRatio = 30.f;
+constexpr int kMaxNu = 4;
+constexpr int kCoefStride = 3 * kMaxNu;   // (sx, sp, sr) per sweep
 
 struct MGLevel {
   int nx, ny, nz, NX, NY, NZ, NN, NE;
@@ -56,11 +70,15 @@ struct MG {
   int nc = 0;                 // coarsest DOFs
   double *A = nullptr, *Y = nullptr, *Ainv = nullptr;
   int maxR = 0;
-  // damped-Jacobi weight per level, omega_l = kOmegaScale / lambda_l with
-  // lambda_l a power-iteration estimate of lambda_max(D^-1 A_l) (device)
+  // per level: lambda_l, a power-iteration estimate of lambda_max(D^-1 A_l),
+  // the first sweep's weight omega_l, and for sweep k = 0 .. nu-1 the
+  // coefficients (sx, sp, sr) of x_{k+1} = sx x_k + sp x_{k-1} + sr D^-1 r_k
+  // at coef[l * kCoefStride + 3 k] (device)
   float* omega = nullptr;
   float* lam = nullptr;
+  float* coef = nullptr;
   int nu = 2;
+  int smoother = 0;           // 0 Chebyshev, 1 damped Jacobi
   bool dirty = true;
   // outer FP64 PCG
   double *x = nullptr, *r = nullptr, *z = nullptr, *q = nullptr, *p[2] = {nullptr, nullptr};
@@ -495,11 +513,13 @@ struct LevelView {
 // (node, output component q, right-hand side r): a CTA is 32 consecutive
 // nodes x (3 R) warps, so each warp reads the stencil rows of its q
 // coalesced and the R warps sharing them hit L1.
-// mode 0: y = b - A x;  mode 1: y = x + omega D^-1 (b - A x);  mode 2: y = D^-1 A x
-// (fixed DOFs of modes 0 and 1 are set to 0; the padding component to 0).
+// mode 0: y = b - A x;  mode 1: y = sx x + sr D^-1 (b - A x);  mode 3: as 1
+// plus sp y_prev (y's previous content);  mode 2: y = D^-1 A x; (sx, sp, sr)
+// a device triple (fixed DOFs of modes 0, 1, 3 are set to 0; the padding
+// component to 0).
 __global__ void __launch_bounds__(768) k_mgs_op(LevelView L, int R, const float* __restrict__ x,
                                                 const float* __restrict__ b, float* y,
-                                                const float* __restrict__ omega_p, int mode) {
+                                                const float* __restrict__ coef, int mode) {
   const int n = blockIdx.x * 32 + threadIdx.x;
   const int q = threadIdx.y % 3, r = threadIdx.y / 3;
   if (n >= L.NN || r >= R) return;
@@ -532,16 +552,19 @@ __global__ void __launch_bounds__(768) k_mgs_op(LevelView L, int R, const float*
     out = di * acc;
   } else {
     out = b[o + q] - acc;
-    if (mode == 1) out = fmaf(__ldg(omega_p) * di, out, x[o + q]);
+    if (mode != 0) {
+      out = fmaf(__ldg(coef + 2) * di, out, __ldg(coef) * x[o + q]);
+      if (mode == 3) out = fmaf(__ldg(coef + 1), y[o + q], out);
+    }
     if ((L.fix[n] >> q) & 1) out = 0.f;
   }
   y[o + q] = out;
   if (q == 0) y[o + 3] = 0.f;
 }
 
-static void launch_mgs_op(const LevelView& L, int R, const float* x, const float* b, float* y, const float* om,
+static void launch_mgs_op(const LevelView& L, int R, const float* x, const float* b, float* y, const float* coef,
                           int mode, cudaStream_t s) {
-  k_mgs_op<<<ceil_div(L.NN, 32), dim3(32, 3 * R), 0, s>>>(L, R, x, b, y, om, mode);
+  k_mgs_op<<<ceil_div(L.NN, 32), dim3(32, 3 * R), 0, s>>>(L, R, x, b, y, coef, mode);
   count_launch();
 }
 
@@ -579,9 +602,16 @@ __global__ void k_mg_scale_dinv(int NN, const float* __restrict__ dinv, float* y
   reinterpret_cast<float4*>(y)[n] = v;
 }
 
-// lambda = ||x_k|| / ||x_{k-1}||, omega = scale / lambda (one CTA)
+// lambda = ||x_k|| / ||x_{k-1}|| and the smoothing coefficients of the
+// level (one CTA).  Chebyshev on [a, b] = [b / kChebRatio, kChebUpper
+// lambda] (Saad, Iterative Methods for Sparse Linear Systems, 2nd ed.,
+// Alg. 12.1, with D^-1 as the preconditioner): theta = (a + b) / 2,
+// delta = (b - a) / 2, sigma = theta / delta, rho_0 = 1 / sigma;
+// x_1 = x_0 + D^-1 r_0 / theta; for k >= 1, rho_k = 1 / (2 sigma - rho_{k-1})
+// and x_{k+1} = x_k + rho_k rho_{k-1} (x_k - x_{k-1}) + (2 rho_k / delta) D^-1 r_k.
+// Damped Jacobi: every sweep x_{k+1} = x_k + omega D^-1 r_k, omega = 1.3333 / lambda.
 __global__ void __launch_bounds__(1024) k_mg_lambda(int NN, const float* __restrict__ xp, const float* __restrict__ xl,
-                                                    float* lam, float* omega, float scale) {
+                                                    float* lam, float* omega, float* coef, int nu, int jacobi) {
   __shared__ double red[2 * 32];
   double v[2] = {0.0, 0.0};
   for (int n = threadIdx.x; n < NN; n += blockDim.x) {
@@ -592,9 +622,26 @@ __global__ void __launch_bounds__(1024) k_mg_lambda(int NN, const float* __restr
   }
   block_sum<2>(v, red);
   if (threadIdx.x == 0) {
-    const double l = (v[0] > 0.0 && v[1] > 0.0) ? sqrt(v[1] / v[0]) : 4.0;
+    const double l = fmax((v[0] > 0.0 && v[1] > 0.0) ? sqrt(v[1] / v[0]) : 4.0, 1e-3);
     *lam = float(l);
-    *omega = float(scale / fmax(l, 1e-3));
+    if (jacobi) {
+      const double w = kOmegaScale / l;
+      *omega = float(w);
+      for (int k = 0; k < nu; ++k) { coef[3 * k] = 1.f; coef[3 * k + 1] = 0.f; coef[3 * k + 2] = float(w); }
+    } else {
+      const double bu = kChebUpper * l, al = bu / kChebRatio;
+      const double th = 0.5 * (bu + al), de = 0.5 * (bu - al), sg = th / de;
+      double rho = 1.0 / sg;
+      *omega = float(1.0 / th);
+      coef[0] = 1.f; coef[1] = 0.f; coef[2] = float(1.0 / th);
+      for (int k = 1; k < nu; ++k) {
+        const double rn = 1.0 / (2.0 * sg - rho);
+        coef[3 * k] = float(1.0 + rn * rho);
+        coef[3 * k + 1] = float(-rn * rho);
+        coef[3 * k + 2] = float(2.0 * rn / de);
+        rho = rn;
+      }
+    }
   }
 }
 
@@ -742,10 +789,13 @@ int mg_create(Ctx& c, int maxR) {
   const size_t V0 = (size_t)c.g.NN * 4 * maxR;
   al(&mg->x, V0); al(&mg->r, V0); al(&mg->z, V0); al(&mg->q, V0); al(&mg->p[0], V0); al(&mg->p[1], V0);
   al(&mg->S, 256); al(&mg->flags, 64); al(&mg->cnt, 16); al(&mg->info, 16);
-  al(&mg->omega, kMaxLevels); al(&mg->lam, kMaxLevels);
+  al(&mg->omega, kMaxLevels); al(&mg->lam, kMaxLevels); al(&mg->coef, kMaxLevels * kCoefStride);
   mg->part_blocks = std::max(c.g.ntiles, 4 * c.num_sms);
   al(&mg->part, (size_t)mg->part_blocks * 3 * 8);
   if (e != cudaSuccess) { c.last_error = std::string("multigrid alloc: ") + cudaGetErrorString(e); return -2; }
+  const char* sm = getenv("TOF_MG_SMOOTHER");
+  mg->smoother = (sm && std::string(sm) == "jacobi") ? 1 : 0;
+  static_assert(kMaxNu >= 2, "smoothing sweeps");
   return 0;
 }
 
@@ -762,7 +812,7 @@ void mg_destroy(Ctx& c) {
   for (auto& g : mg->vexec)
     if (g) cudaGraphExecDestroy(g);
   void* ps[] = {mg->A, mg->Y, mg->Ainv, mg->x, mg->r, mg->z, mg->q, mg->p[0], mg->p[1], mg->S, mg->flags, mg->cnt,
-                mg->info, mg->part, mg->omega, mg->lam};
+                mg->info, mg->part, mg->omega, mg->lam, mg->coef};
   for (void* p : ps)
     if (p) cudaFree(p);
   delete mg;
@@ -816,7 +866,8 @@ int mg_setup(Ctx& c, cudaStream_t s) {
       }
       std::swap(x, y);
     }
-    k_mg_lambda<<<1, 1024, 0, s>>>(V.NN, y, x, mg->lam + k, mg->omega + k, kOmegaScale);
+    k_mg_lambda<<<1, 1024, 0, s>>>(V.NN, y, x, mg->lam + k, mg->omega + k, mg->coef + k * kCoefStride, mg->nu,
+                                   mg->smoother);
     count_launch();
   }
   mg->dirty = false;
@@ -841,12 +892,14 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
   // downward
   for (int k = 0; k < nl - 1; ++k) {
     MGLevel& L = mg->L[k];
-    const float* om = mg->omega + k;
-    k_mg_jacobi0<<<ceil_div(L.NN * R, 256), 256, 0, s>>>(L.NN, R, L.dinv, L.r, cur[k], om);
+    const float* cf = mg->coef + k * kCoefStride;
+    // sweep 0 from x = 0: x_1 = sr D^-1 r
+    k_mg_jacobi0<<<ceil_div(L.NN * R, 256), 256, 0, s>>>(L.NN, R, L.dinv, L.r, cur[k], cf + 2);
     count_launch();
     for (int sw = 1; sw < mg->nu; ++sw) {
-      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
-      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], om, 1, s);
+      const bool prev = sw >= 2;             // x_0 = 0: sweep 1 has no x_{k-1} term
+      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, cf + 3 * sw, prev, R, s)) return -2; }
+      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], cf + 3 * sw, prev ? 3 : 1, s);
       std::swap(cur[k], alt[k]);
     }
     if (k == 0) { if (launch_matvec(c, 0, false, cur[k], L.t, R, L.r, s)) return -2; }
@@ -866,10 +919,11 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
     MGLevel& C = mg->L[k + 1];
     k_mg_prolong<<<grid1(L.NN * R), 128, 0, s>>>(transfer(L, C), R, cur[k + 1], L.fix, cur[k]);
     count_launch();
-    const float* om = mg->omega + k;
+    const float* cf = mg->coef + k * kCoefStride;
     for (int sw = 0; sw < mg->nu; ++sw) {
-      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, om, R, s)) return -2; }
-      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], om, 1, s);
+      const bool prev = sw >= 1;             // alt holds x_{k-1} after the first sweep
+      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, cf + 3 * sw, prev, R, s)) return -2; }
+      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], cf + 3 * sw, prev ? 3 : 1, s);
       std::swap(cur[k], alt[k]);
     }
   }

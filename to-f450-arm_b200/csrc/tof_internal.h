@@ -101,8 +101,8 @@ void launch_factors(Ctx& c, const double* rho, cudaStream_t s);
 void launch_diag(Ctx& c, cudaStream_t s);
 int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, const void* b_residual,
                   cudaStream_t s);
-int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* omega, int R,
-                   cudaStream_t s);
+int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* coef, bool prev,
+                   int R, cudaStream_t s);
 void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s);
 void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s);
 void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s);

@@ -94,8 +94,12 @@ struct MatvecArgs {
   const T* b;          // residual mode: rhs, else null
   T* y;
   long long vstride;   // elements between consecutive vectors (NN*4)
-  const T* dinv;       // smoother mode (with b): y = x + omega D^-1 (b - A x)
-  const float* omega;  // device scalar (smoother mode)
+  // smoother mode (with b): y = sx x + sp y_prev + sr D^-1 (b - A x), the
+  // coefficients (sx, sp, sr) a device triple; y_prev (the output buffer's
+  // previous content, own node only) is read only with prev
+  const T* dinv;
+  const float* coef;
+  bool prev;
 };
 
 template <typename T, int R>
@@ -139,10 +143,17 @@ __global__ void __launch_bounds__(512) k_matvec(const __grid_constant__ CUtensor
       if (a.dinv) {
         const V4 xc = halo_center<T>(sx, tg, r, tx, ty, tz);
         const V4 di = reinterpret_cast<const V4*>(a.dinv)[n];
-        const T om = T(__ldg(a.omega));
-        out.x = fma(om * di.x, out.x, xc.x);
-        out.y = fma(om * di.y, out.y, xc.y);
-        out.z = fma(om * di.z, out.z, xc.z);
+        const T cx = T(__ldg(a.coef)), cr = T(__ldg(a.coef + 2));
+        out.x = fma(cr * di.x, out.x, cx * xc.x);
+        out.y = fma(cr * di.y, out.y, cx * xc.y);
+        out.z = fma(cr * di.z, out.z, cx * xc.z);
+        if (a.prev) {
+          const T cp = T(__ldg(a.coef + 1));
+          const V4 yp = reinterpret_cast<const V4*>(a.y + r * a.vstride)[n];
+          out.x = fma(cp, yp.x, out.x);
+          out.y = fma(cp, yp.y, out.y);
+          out.z = fma(cp, yp.z, out.z);
+        }
       }
     } else {
       out.x = acc[r][0]; out.y = acc[r][1]; out.z = acc[r][2];
@@ -157,7 +168,7 @@ __global__ void __launch_bounds__(512) k_matvec(const __grid_constant__ CUtensor
 
 template <typename T, int R>
 static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b, cudaStream_t s,
-                           const void* dinv = nullptr, const float* omega = nullptr) {
+                           const void* dinv = nullptr, const float* coef = nullptr, bool prev = false) {
   CUtensorMap tm;
   std::string err;
   if (!encode_node4_map(&tm, x, c.g, R, sizeof(T) == 8, &err)) {
@@ -177,7 +188,8 @@ static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b
   a.y = reinterpret_cast<T*>(y);
   a.vstride = (long long)c.g.NN * 4;
   a.dinv = reinterpret_cast<const T*>(dinv);
-  a.omega = omega;
+  a.coef = coef;
+  a.prev = prev;
   const TileGeom tg{0, 0, 0, c.g.TX + 2, c.g.TY + 2, c.g.TZ + 2, c.g.TX + 1, c.g.TY + 1, c.g.TZ + 1};
   size_t smem = halo_bytes<T>(c.g, R) + sizeof(T) * (kKeBlocksLen + tg.EX * tg.EY * tg.EZ);
   smem = ((smem + 15) & ~size_t(15)) + 16;
@@ -221,14 +233,15 @@ int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, co
   return 0;
 }
 
-// y = x + omega D^-1 (b - K x) on the fine level, FP32, R in {1,2,4,8}
-int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* omega, int R,
-                   cudaStream_t s) {
+// y = sx x + sp y_prev + sr D^-1 (b - K x) on the fine level, FP32, R in
+// {1,2,4,8}; coef = device (sx, sp, sr), y_prev read only with prev
+int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* coef, bool prev,
+                   int R, cudaStream_t s) {
   switch (R) {
-    case 8: return matvec_launch_t<float, 8>(c, 0, x, y, b, s, dinv, omega);
-    case 4: return matvec_launch_t<float, 4>(c, 0, x, y, b, s, dinv, omega);
-    case 2: return matvec_launch_t<float, 2>(c, 0, x, y, b, s, dinv, omega);
-    default: return matvec_launch_t<float, 1>(c, 0, x, y, b, s, dinv, omega);
+    case 8: return matvec_launch_t<float, 8>(c, 0, x, y, b, s, dinv, coef, prev);
+    case 4: return matvec_launch_t<float, 4>(c, 0, x, y, b, s, dinv, coef, prev);
+    case 2: return matvec_launch_t<float, 2>(c, 0, x, y, b, s, dinv, coef, prev);
+    default: return matvec_launch_t<float, 1>(c, 0, x, y, b, s, dinv, coef, prev);
   }
 }
 
