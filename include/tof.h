@@ -91,7 +91,16 @@ const char* tof_last_error(const tof_ctx* ctx);   /* ctx may be NULL: last creat
  * mass_kg / n_nodes on each DOF of the tip nodes (src/fem.py:383-398).
  * `tile` (node tile x, y, z; NULL = default 8x4x4) must have x*y*z <= 256.
  * max_rhs / max_modes (1..8) size the solver workspace; this is the only
- * call that allocates device memory. */
+ * call that allocates device memory.
+ * Concurrency: calls on one context are issued in order on their streams,
+ * except that one call of the static family (tof_pcg, tof_elem_quadform,
+ * tof_compliance_sens) and one of the modal family (tof_lobpcg with the
+ * Jacobi or multigrid preconditioner, tof_eig_sens, tof_effective_mass) may
+ * run at the same time from two host threads on two streams: the families
+ * keep separate scratch and multigrid vectors.  Both streams must first wait
+ * on the stream that set the density (and, for the multigrid, ran
+ * tof_mg_setup).  The error message of tof_last_error may then come from
+ * either call. */
 int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[576], const double Me[576],
                    const uint8_t* active, const uint8_t* fixed_dof, const double* tip_lump,
                    const tof_simp_params* simp, int max_rhs, int max_modes, const int tile[3], tof_ctx** out);
@@ -139,6 +148,11 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
 int tof_mg_query(tof_ctx* ctx, int level, int* dims, float* omega, void* stream);
 int tof_mg_export(tof_ctx* ctx, int level, float* out, void* stream);
 int tof_mg_apply(tof_ctx* ctx, const float* r, float* e, int R, void* stream);
+/* Build the multigrid hierarchy for the current density now, on `stream`
+ * (otherwise the first solve that needs it builds it on its own stream).
+ * Call it before issuing a static and a modal solve on two streams that both
+ * wait on `stream` (see the concurrency note at tof_ctx_create). */
+int tof_mg_setup(tof_ctx* ctx, void* stream);
 
 /* Lowest `nmodes` eigenpairs of K_ff x = lam M_ff x with a block of `block`
  * vectors (nmodes <= block <= 8).  X (device node4 FP64, `block` vectors)

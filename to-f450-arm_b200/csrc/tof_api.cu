@@ -120,7 +120,8 @@ static void free_ctx(Ctx& c) {
   mg_destroy(c);
   void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
                   c.fK64, c.fM64, c.fK32, c.fM32, c.rho, c.dK64, c.dM64, c.dinvK64, c.dinvK32, c.partials,
-                  c.bar, c.status, c.scal, c.counters, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part};
+                  c.bar, c.status, c.scal, c.counters, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part,
+                  c.gram_part_m, c.counters_m, c.status_m, c.scal_m};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -256,6 +257,8 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.lw64, 21 * MM * V));
   A(dalloc(c, &c.gram, 8 * 576));
   A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 1152));
+  A(dalloc(c, &c.gram_part_m, (size_t)c.gram_blocks * 1152));
+  A(dalloc(c, &c.counters_m, 16)); A(dalloc(c, &c.status_m, 16)); A(dalloc(c, &c.scal_m, 256));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
   if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error);
   A(cudaMemcpy(c.Ke64, Ke, 576 * 8, cudaMemcpyHostToDevice));
@@ -530,6 +533,13 @@ int tof_mg_export(tof_ctx* ctx, int level, float* out, void* stream) {
   return r == -1 ? TOF_ERR_ARG : r == -2 ? TOF_ERR_CUDA : TOF_OK;
 }
 
+int tof_mg_setup(tof_ctx* ctx, void* stream) {
+  if (!ctx) return TOF_ERR_ARG;
+  Ctx& c = ctx->c;
+  if (mg_ensure(c, (cudaStream_t)stream)) { c.last_error = "tof_mg_setup: multigrid setup failed"; return TOF_ERR_CUDA; }
+  return TOF_OK;
+}
+
 int tof_mg_apply(tof_ctx* ctx, const float* r, float* e, int R, void* stream) {
   if (!ctx || !r || !e) return TOF_ERR_ARG;
   const int rc = mg_apply(ctx->c, r, e, R, (cudaStream_t)stream);
@@ -589,7 +599,7 @@ int tof_eig_sens(tof_ctx* ctx, const double* qK, const double* qM, double lam, d
                  void* stream) {
   if (!ctx || !qK || !qM || !out) return TOF_ERR_ARG;
   Ctx& c = ctx->c;
-  launch_eig_sens(c.g.NE, c.rho, qK, qM, c.active, c.sp, lam, vMv_tip, out, c.gram_part, c.scal + 128,
+  launch_eig_sens(c.g.NE, c.rho, qK, qM, c.active, c.sp, lam, vMv_tip, out, c.gram_part_m, c.scal_m,
                   (cudaStream_t)stream);
   CUDA_TRY(cudaGetLastError());
   return TOF_OK;
@@ -647,7 +657,7 @@ int tof_effective_mass(tof_ctx* ctx, const double* modes, int nmodes, int direct
     CUDA_TRY(cudaStreamSynchronize(s));
   }
   if (launch_matvec(c, 1, true, A, MA, nmodes + 1, nullptr, s)) return TOF_ERR_CUDA;
-  launch_gram(c, true, A, nmodes + 1, MA, nmodes + 1, c.gram + 6 * 576, s);
+  launch_gram(c, true, A, nmodes + 1, MA, nmodes + 1, c.gram + 6 * 576, s, c.gram_part_m);
   double G[81];
   CUDA_TRY(cudaMemcpyAsync(G, c.gram + 6 * 576, sizeof(double) * (nmodes + 1) * (nmodes + 1),
                            cudaMemcpyDeviceToHost, s));

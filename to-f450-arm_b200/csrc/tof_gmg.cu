@@ -61,12 +61,19 @@ struct MGLevel {
   float* St = nullptr;     // [243][NN] assembled node stencils (levels 1 .. nlev-2)
   float* dinv = nullptr;   // node4
   uint8_t* fix = nullptr;  // node bits
-  float *r = nullptr, *e = nullptr, *e2 = nullptr, *t = nullptr;   // node4 x maxR
 };
+
+// V-cycle vectors of one level (node4 x maxR): right-hand side, correction
+// and its ping-pong partner, residual
+struct MGBuf {
+  float *r = nullptr, *e = nullptr, *e2 = nullptr, *t = nullptr;
+};
+constexpr int kLanes = 2;      // lane 0: static solves, lane 1: modal solves
 
 struct MG {
   int nlev = 0;
   MGLevel L[kMaxLevels];
+  MGBuf buf[kLanes][kMaxLevels];
   int nc = 0;                 // coarsest DOFs
   double *A = nullptr, *Y = nullptr, *Ainv = nullptr;
   int maxR = 0;
@@ -92,9 +99,9 @@ struct MG {
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t gnodes[4] = {0, 0, 0, 0};
   bool graph_failed = false;
-  // a single V-cycle per R, replayed by callers outside the PCG graphs
-  cudaGraphExec_t vexec[4] = {nullptr, nullptr, nullptr, nullptr};
-  size_t vnodes[4] = {0, 0, 0, 0};
+  // a single V-cycle per lane and R, replayed by callers outside the PCG graphs
+  cudaGraphExec_t vexec[kLanes][4] = {};
+  size_t vnodes[kLanes][4] = {};
   bool vgraph_failed = false;
 };
 constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
@@ -782,7 +789,10 @@ int mg_create(Ctx& c, int maxR) {
       L.dinv = c.dinvK32;
       L.fix = c.fix;
     }
-    al(&L.r, V); al(&L.e, V); al(&L.e2, V); al(&L.t, V);
+    for (int ln = 0; ln < kLanes; ++ln) {
+      MGBuf& B = mg->buf[ln][k];
+      al(&B.r, V); al(&B.e, V); al(&B.e2, V); al(&B.t, V);
+    }
   }
   const size_t n2 = (size_t)mg->nc * mg->nc;
   al(&mg->A, n2); al(&mg->Y, n2); al(&mg->Ainv, n2);
@@ -805,12 +815,16 @@ void mg_destroy(Ctx& c) {
   for (int k = 0; k < mg->nlev; ++k) {
     MGLevel& L = mg->L[k];
     if (k > 0) { cudaFree(L.Ae); cudaFree(L.dinv); cudaFree(L.fix); if (L.St) cudaFree(L.St); }
-    cudaFree(L.r); cudaFree(L.e); cudaFree(L.e2); cudaFree(L.t);
+    for (int ln = 0; ln < kLanes; ++ln) {
+      MGBuf& B = mg->buf[ln][k];
+      cudaFree(B.r); cudaFree(B.e); cudaFree(B.e2); cudaFree(B.t);
+    }
   }
   for (auto& g : mg->gexec)
     if (g) cudaGraphExecDestroy(g);
-  for (auto& g : mg->vexec)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto& lane : mg->vexec)
+    for (auto& g : lane)
+      if (g) cudaGraphExecDestroy(g);
   void* ps[] = {mg->A, mg->Y, mg->Ainv, mg->x, mg->r, mg->z, mg->q, mg->p[0], mg->p[1], mg->S, mg->flags, mg->cnt,
                 mg->info, mg->part, mg->omega, mg->lam, mg->coef};
   for (void* p : ps)
@@ -852,8 +866,8 @@ int mg_setup(Ctx& c, cudaStream_t s) {
   // smoothing weights: power iteration on D^-1 A_l (scratch: the level's e, e2)
   for (int k = 0; k < mg->nlev - 1; ++k) {
     MGLevel& V = mg->L[k];
-    float* x = V.e;
-    float* y = V.e2;
+    float* x = mg->buf[0][k].e;
+    float* y = mg->buf[0][k].e2;
     k_mg_power_init<<<ceil_div(V.NN, 256), 256, 0, s>>>(V.NN, V.fix, x);
     count_launch();
     for (int it = 0; it < kPowerIters; ++it) {
@@ -875,43 +889,44 @@ int mg_setup(Ctx& c, cudaStream_t s) {
 }
 
 template <int R>
-static int vcycle_t(Ctx& c, cudaStream_t s) {
+static int vcycle_t(Ctx& c, int lane, cudaStream_t s) {
   MG* mg = c.mg;
+  MGBuf* Bf = mg->buf[lane];
   const int nl = mg->nlev;
   auto grid1 = [](int n) { return ceil_div(n, 128); };
-  // Jacobi sweeps ping-pong between e and e2; the first sweep writes to
-  // whichever buffer makes the last sweep of the level land in L.e, so the
+  // Smoothing sweeps ping-pong between e and e2; the first sweep writes to
+  // whichever buffer makes the last sweep of the level land in e, so the
   // buffer roles are the same in every V-cycle (required for graph replay).
   float* cur[kMaxLevels];
   float* alt[kMaxLevels];
   for (int k = 0; k < nl; ++k) {
     const bool odd = ((2 * mg->nu - 1) & 1) != 0;   // sweeps after the first
-    cur[k] = odd ? mg->L[k].e2 : mg->L[k].e;
-    alt[k] = odd ? mg->L[k].e : mg->L[k].e2;
+    cur[k] = odd ? Bf[k].e2 : Bf[k].e;
+    alt[k] = odd ? Bf[k].e : Bf[k].e2;
   }
   // downward
   for (int k = 0; k < nl - 1; ++k) {
     MGLevel& L = mg->L[k];
     const float* cf = mg->coef + k * kCoefStride;
     // sweep 0 from x = 0: x_1 = sr D^-1 r
-    k_mg_jacobi0<<<ceil_div(L.NN * R, 256), 256, 0, s>>>(L.NN, R, L.dinv, L.r, cur[k], cf + 2);
+    k_mg_jacobi0<<<ceil_div(L.NN * R, 256), 256, 0, s>>>(L.NN, R, L.dinv, Bf[k].r, cur[k], cf + 2);
     count_launch();
     for (int sw = 1; sw < mg->nu; ++sw) {
       const bool prev = sw >= 2;             // x_0 = 0: sweep 1 has no x_{k-1} term
-      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, cf + 3 * sw, prev, R, s)) return -2; }
-      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], cf + 3 * sw, prev ? 3 : 1, s);
+      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], Bf[k].r, L.dinv, cf + 3 * sw, prev, R, s)) return -2; }
+      else launch_mgs_op(view(L), R, cur[k], Bf[k].r, alt[k], cf + 3 * sw, prev ? 3 : 1, s);
       std::swap(cur[k], alt[k]);
     }
-    if (k == 0) { if (launch_matvec(c, 0, false, cur[k], L.t, R, L.r, s)) return -2; }
-    else launch_mgs_op(view(L), R, cur[k], L.r, L.t, nullptr, 0, s);
+    if (k == 0) { if (launch_matvec(c, 0, false, cur[k], Bf[k].t, R, Bf[k].r, s)) return -2; }
+    else launch_mgs_op(view(L), R, cur[k], Bf[k].r, Bf[k].t, nullptr, 0, s);
     MGLevel& C = mg->L[k + 1];
-    k_mg_restrict<<<grid1(C.NN * R), 128, 0, s>>>(transfer(L, C), R, L.t, C.fix, C.r);
+    k_mg_restrict<<<grid1(C.NN * R), 128, 0, s>>>(transfer(L, C), R, Bf[k].t, C.fix, Bf[k + 1].r);
     count_launch();
   }
   {
     MGLevel& L = mg->L[nl - 1];
-    launch_coarse_solve(L.NN, R, mg->Ainv, L.r, L.e, s);
-    cur[nl - 1] = L.e;
+    launch_coarse_solve(L.NN, R, mg->Ainv, Bf[nl - 1].r, Bf[nl - 1].e, s);
+    cur[nl - 1] = Bf[nl - 1].e;
   }
   // upward
   for (int k = nl - 2; k >= 0; --k) {
@@ -922,58 +937,60 @@ static int vcycle_t(Ctx& c, cudaStream_t s) {
     const float* cf = mg->coef + k * kCoefStride;
     for (int sw = 0; sw < mg->nu; ++sw) {
       const bool prev = sw >= 1;             // alt holds x_{k-1} after the first sweep
-      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], L.r, L.dinv, cf + 3 * sw, prev, R, s)) return -2; }
-      else launch_mgs_op(view(L), R, cur[k], L.r, alt[k], cf + 3 * sw, prev ? 3 : 1, s);
+      if (k == 0) { if (launch_smooth0(c, cur[k], alt[k], Bf[k].r, L.dinv, cf + 3 * sw, prev, R, s)) return -2; }
+      else launch_mgs_op(view(L), R, cur[k], Bf[k].r, alt[k], cf + 3 * sw, prev ? 3 : 1, s);
       std::swap(cur[k], alt[k]);
     }
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-static int vcycle_eager(Ctx& c, int R, cudaStream_t s) {
+static int vcycle_eager(Ctx& c, int R, int lane, cudaStream_t s) {
   if (c.mg->nlev == 1) {
     MGLevel& L = c.mg->L[0];
-    launch_coarse_solve(L.NN, R, c.mg->Ainv, L.r, L.e, s);
+    launch_coarse_solve(L.NN, R, c.mg->Ainv, c.mg->buf[lane][0].r, c.mg->buf[lane][0].e, s);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
   }
   switch (R) {
-    case 1: return vcycle_t<1>(c, s);
-    case 2: return vcycle_t<2>(c, s);
-    case 4: return vcycle_t<4>(c, s);
-    case 8: return vcycle_t<8>(c, s);
+    case 1: return vcycle_t<1>(c, lane, s);
+    case 2: return vcycle_t<2>(c, lane, s);
+    case 4: return vcycle_t<4>(c, lane, s);
+    case 8: return vcycle_t<8>(c, lane, s);
   }
   return -1;
 }
 
-// Apply the V-cycle to mg->L[0].r (R vectors); result in mg->L[0].e.  Inside
-// a stream capture (the PCG graphs) the kernels are recorded as they are;
-// otherwise the cycle for this R is captured once and replayed as a graph,
-// which removes the per-kernel launch overhead of ~40 short launches (the
-// buffers, tensor maps and smoothing weights it references never move).
-int mg_vcycle(Ctx& c, int R, cudaStream_t s) {
+// Apply the V-cycle to mg_rhs(c, lane) (R vectors); result in mg_out(c, lane).
+// Inside a stream capture (the PCG graphs) the kernels are recorded as they
+// are; otherwise the cycle for this lane and R is captured once and replayed
+// as a graph, which removes the per-kernel launch overhead of ~40 short
+// launches (the buffers, tensor maps and smoothing coefficients it references
+// never move).
+int mg_vcycle(Ctx& c, int R, cudaStream_t s, int lane) {
   MG* mg = c.mg;
   const int ri = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : -1;
-  if (ri < 0) return -1;
-  if (capturing() || mg->vgraph_failed) return vcycle_eager(c, R, s);
-  if (!mg->vexec[ri]) {
+  if (ri < 0 || lane < 0 || lane >= kLanes) return -1;
+  if (capturing() || mg->vgraph_failed) return vcycle_eager(c, R, lane, s);
+  cudaGraphExec_t& ge = mg->vexec[lane][ri];
+  if (!ge) {
     cudaGraph_t graph = nullptr;
     bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     capturing() = ok;
-    if (ok) ok = vcycle_eager(c, R, s) == 0;
+    if (ok) ok = vcycle_eager(c, R, lane, s) == 0;
     capturing() = false;
     const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
-    if (ok && ended && graph && cudaGraphInstantiate(&mg->vexec[ri], graph, 0) == cudaSuccess) {
-      cudaGraphGetNodes(graph, nullptr, &mg->vnodes[ri]);
+    if (ok && ended && graph && cudaGraphInstantiate(&ge, graph, 0) == cudaSuccess) {
+      cudaGraphGetNodes(graph, nullptr, &mg->vnodes[lane][ri]);
     } else {
-      mg->vexec[ri] = nullptr;
+      ge = nullptr;
       mg->vgraph_failed = true;
     }
     if (graph) cudaGraphDestroy(graph);
     cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
-    if (!mg->vexec[ri]) return vcycle_eager(c, R, s);
+    if (!ge) return vcycle_eager(c, R, lane, s);
   }
-  if (cudaGraphLaunch(mg->vexec[ri], s) != cudaSuccess) return -2;
-  count_launch((long long)mg->vnodes[ri]);
+  if (cudaGraphLaunch(ge, s) != cudaSuccess) return -2;
+  count_launch((long long)mg->vnodes[lane][ri]);
   return 0;
 }
 
@@ -1010,17 +1027,17 @@ int mg_apply(Ctx& c, const float* r, float* e, int R, cudaStream_t s) {
   if (R > mg->maxR) return -1;
   if (mg->dirty && mg_setup(c, s)) return -2;
   const size_t bytes = sizeof(float) * 4 * (size_t)c.g.NN * R;
-  cudaMemcpyAsync(mg->L[0].r, r, bytes, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(mg->buf[0][0].r, r, bytes, cudaMemcpyDeviceToDevice, s);
   if (mg_vcycle(c, R, s)) return -2;
-  return cudaMemcpyAsync(e, mg->L[0].e, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -2;
+  return cudaMemcpyAsync(e, mg->buf[0][0].e, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -2;
 }
 
 void mg_mark_dirty(Ctx& c) {
   if (c.mg) c.mg->dirty = true;
 }
 int mg_ensure(Ctx& c, cudaStream_t s) { return c.mg->dirty ? mg_setup(c, s) : 0; }
-float* mg_rhs(Ctx& c) { return c.mg->L[0].r; }
-float* mg_out(Ctx& c) { return c.mg->L[0].e; }
+float* mg_rhs(Ctx& c, int lane) { return c.mg->buf[lane][0].r; }
+float* mg_out(Ctx& c, int lane) { return c.mg->buf[lane][0].e; }
 int mg_levels(const Ctx& c) { return c.mg ? c.mg->nlev : 0; }
 
 // ---------------------------------------------------------------------------
@@ -1231,11 +1248,11 @@ static int mgpcg_iter(Ctx& c, int pc, cudaStream_t s) {
   kern<<<c.g.ntiles, c.g.TX * c.g.TY * c.g.TZ, smem, s>>>(tmz, tmp, c.g, c.fK64, c.keb64, c.fix, mg->p[pc ^ 1], mg->q,
                                                            mg->S, mg->flags, mg->part, mg->cnt + 0);
   count_launch();
-  k_mgpcg_xr<R><<<eb, 256, 0, s>>>(c.g.NN, mg->p[pc ^ 1], mg->q, mg->x, mg->r, mg->L[0].r, mg->S, mg->flags, mg->part,
+  k_mgpcg_xr<R><<<eb, 256, 0, s>>>(c.g.NN, mg->p[pc ^ 1], mg->q, mg->x, mg->r, mg->buf[0][0].r, mg->S, mg->flags, mg->part,
                                    mg->cnt + 1);
   count_launch();
   if (mg_vcycle(c, R, s)) return -2;
-  k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->L[0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 0);
+  k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->buf[0][0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 0);
   count_launch();
   return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -1252,11 +1269,11 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
   cudaMemcpyAsync(mg->x, x, sizeof(double) * R * V, cudaMemcpyDeviceToDevice, s);
   if (launch_matvec(c, 0, true, mg->x, mg->r, R, b, s)) return -2;
   const int eb = std::min(ceil_div(c.g.NN, 256), 2 * c.num_sms);
-  k_mgpcg_init<R><<<eb, 256, 0, s>>>(c.g.NN, b, mg->r, mg->L[0].r, mg->p[0], mg->S, mg->flags, mg->part, mg->cnt + 3,
+  k_mgpcg_init<R><<<eb, 256, 0, s>>>(c.g.NN, b, mg->r, mg->buf[0][0].r, mg->p[0], mg->S, mg->flags, mg->part, mg->cnt + 3,
                                      rtol);
   count_launch();
   if (mg_vcycle(c, R, s)) return -2;
-  k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->L[0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 1);
+  k_mgpcg_zrz<R><<<eb, 256, 0, s>>>(c.g.NN, mg->buf[0][0].e, mg->r, mg->z, mg->S, mg->flags, mg->part, mg->cnt + 2, 1);
   count_launch();
   int it = 0;
   int hf[9];

@@ -81,6 +81,15 @@ struct Ctx {
   double* gram = nullptr;      // [2][24*24] + small-eig outputs
   double* gram_part = nullptr; // [gram blocks][24*24]
   int gram_blocks = 0;
+  // Scratch of the modal family (LOBPCG, eigenvalue sensitivities, effective
+  // masses), apart from the static family's (PCG, true residuals, compliance
+  // sensitivities), so one solve of each family may run at the same time on
+  // two streams.  The multigrid V-cycle keeps one set of level vectors per
+  // family (lane 0 static, lane 1 modal).
+  double* gram_part_m = nullptr; // [gram blocks][24*24]
+  unsigned* counters_m = nullptr; // [16]
+  int* status_m = nullptr;       // [16]
+  double* scal_m = nullptr;      // [256]
 
   // persistent-launch capacity for each kernel flavour
   int coop_pipe[9] = {0};
@@ -105,7 +114,7 @@ int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float
                    int R, cudaStream_t s);
 void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s);
 void launch_unpack(const Ctx& c, const void* src, bool f64, double* dst, long long ld, int nvec, cudaStream_t s);
-void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s);
+void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s, double* part = nullptr);
 // Column selection of a node4 block: vector k of the selection is vector
 // col[k] of the block (up to 24).
 struct ColMap {
@@ -113,10 +122,10 @@ struct ColMap {
 };
 // G1 = A[:, cols]^T B1[:, cols], G2 = A[:, cols]^T B2[:, cols] (n x n) in one pass
 void launch_gram2_cols(Ctx& c, bool f64, const void* A, const void* B1, const void* B2, const ColMap& cols, int n,
-                       double* G1, double* G2, cudaStream_t s);
+                       double* G1, double* G2, cudaStream_t s, double* part = nullptr);
 // G = A[:, ma]^T B[:, mb] (na x nb), same kernels as launch_gram
 void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na, const void* B, const ColMap& mb,
-                      int nb, double* G, cudaStream_t s);
+                      int nb, double* G, cudaStream_t s, double* part = nullptr);
 void launch_quadform(const Ctx& c, int op, bool f64, const void* v, int nvec, double* out, cudaStream_t s);
 void launch_convert(const void* src, bool src64, void* dst, bool dst64, long long n, cudaStream_t s);
 void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s);
@@ -148,9 +157,9 @@ void mg_destroy(Ctx& c);
 int mg_setup(Ctx& c, cudaStream_t s);
 void mg_mark_dirty(Ctx& c);
 int mg_ensure(Ctx& c, cudaStream_t s);
-int mg_vcycle(Ctx& c, int R, cudaStream_t s);   // mg_rhs -> mg_out
-float* mg_rhs(Ctx& c);
-float* mg_out(Ctx& c);
+int mg_vcycle(Ctx& c, int R, cudaStream_t s, int lane = 0);   // mg_rhs -> mg_out
+float* mg_rhs(Ctx& c, int lane = 0);
+float* mg_out(Ctx& c, int lane = 0);
 int mg_levels(const Ctx& c);
 int mg_query(Ctx& c, int level, int* dims, float* omega, cudaStream_t s);
 int mg_export(Ctx& c, int level, float* out, cudaStream_t s);

@@ -483,43 +483,46 @@ __global__ void __launch_bounds__(256) k_gram2_reduce(int nblocks, int npair, co
 }
 
 void launch_gram2_cols(Ctx& c, bool f64, const void* A, const void* B1, const void* B2, const ColMap& cols, int n,
-                       double* G1, double* G2, cudaStream_t s) {
+                       double* G1, double* G2, cudaStream_t s, double* part) {
+  if (!part) part = c.gram_part;
   const int nchunks = ceil_div(c.g.NN, kGram2Chunk);
   int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
   if (blocks < 1) blocks = 1;
   const long long vs = (long long)c.g.NN * 4;
   if (f64)
     k_gram2_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, (const double*)B1,
-                                                           (const double*)B2, cols, n, vs, c.gram_part);
+                                                           (const double*)B2, cols, n, vs, part);
   else
     k_gram2_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, (const float*)B1,
-                                                          (const float*)B2, cols, n, vs, c.gram_part);
+                                                          (const float*)B2, cols, n, vs, part);
   count_launch();
-  k_gram2_reduce<<<ceil_div(2 * n * n, 8), 256, 0, s>>>(blocks, n * n, c.gram_part, G1, G2);
+  k_gram2_reduce<<<ceil_div(2 * n * n, 8), 256, 0, s>>>(blocks, n * n, part, G1, G2);
   count_launch();
 }
 
 void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na, const void* B, const ColMap& mb,
-                      int nb, double* G, cudaStream_t s) {
+                      int nb, double* G, cudaStream_t s, double* part) {
+  if (!part) part = c.gram_part;
   const int nchunks = ceil_div(c.g.NN, kGramChunk);
   int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
   if (blocks < 1) blocks = 1;
   const long long vs = (long long)c.g.NN * 4;
   if (f64)
     k_gram_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, ma, na, (const double*)B, mb,
-                                                          nb, vs, c.gram_part);
+                                                          nb, vs, part);
   else
     k_gram_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, ma, na, (const float*)B, mb, nb,
-                                                         vs, c.gram_part);
+                                                         vs, part);
   count_launch();
-  k_gram_reduce<<<ceil_div(na * nb, 8), 256, 0, s>>>(blocks, na * nb, c.gram_part, G);
+  k_gram_reduce<<<ceil_div(na * nb, 8), 256, 0, s>>>(blocks, na * nb, part, G);
   count_launch();
 }
 
-void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s) {
+void launch_gram(Ctx& c, bool f64, const void* A, int na, const void* B, int nb, double* G, cudaStream_t s,
+                 double* part) {
   ColMap id;
   for (int k = 0; k < 24; ++k) id.col[k] = k;
-  launch_gram_cols(c, f64, A, id, na, B, id, nb, G, s);
+  launch_gram_cols(c, f64, A, id, na, B, id, nb, G, s, part);
 }
 
 // ---------------------------------------------------------------------------

@@ -469,7 +469,7 @@ static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s) {
   double* GM = c.gram + 576;
   double* C = c.gram + 2 * 576;
   double* th = c.gram + 3 * 576;
-  int* info = c.status + 8;
+  int* info = c.status_m;
   k_small_eig<<<1, kEigThreads, 0, s>>>(n, m, GK, GM, drop, C, th, info);
   count_launch();
   return 0;
@@ -501,7 +501,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   double* C = c.gram + 2 * 576;
   double* th = c.gram + 3 * 576;
   double* rn = c.gram + 3 * 576 + 32;
-  int* info = c.status + 8;
+  int* info = c.status_m;
   const int rblocks = 2 * c.num_sms;
   int cur = 0;
   if (precond == 2 && mg_ensure(c, s)) return -2;
@@ -510,7 +510,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
   if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
   // initial Rayleigh-Ritz on X alone
-  launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], identity_cols(), nb, GK, GM, s);
+  launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], identity_cols(), nb, GK, GM, s, c.gram_part_m);
   lob_small_eig(c, nb, nb, drop, s);
   const ColMap ident = identity_cols();
   launch_lob_update<T>(NN, nb, nb, ident, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C, (T*)B.S[cur ^ 1],
@@ -560,7 +560,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
     k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, (T*)B.S[cur],
-                                           wslot, c.gram_part, c.counters, rn);
+                                           wslot, c.gram_part_m, c.counters_m, rn);
     count_launch();
     cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
@@ -628,11 +628,11 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (precond == 2) {
       // W <- V-cycle(W): the FP32 multigrid approximation of K^-1
       if (mg_ensure(c, s)) return -2;
-      float* r32 = mg_rhs(c);
+      float* r32 = mg_rhs(c, 1);
       if (R > na) cudaMemsetAsync(r32, 0, sizeof(float) * R * vs, s);
       launch_convert(W, f64, r32, false, (long long)na * vs, s);
-      if (mg_vcycle(c, R, s)) return -2;
-      launch_convert(mg_out(c), false, W, f64, (long long)na * vs, s);
+      if (mg_vcycle(c, R, s, 1)) return -2;
+      launch_convert(mg_out(c, 1), false, W, f64, (long long)na * vs, s);
     } else if (precond == 1) {
       // W <- (inexact) K^-1 W by block PCG (FP32)
       const size_t pblk = (size_t)c.max_rhs * vs;
@@ -654,7 +654,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (it > 0)
       for (int k = 0; k < na; ++k) cols.col[ncols++] = 2 * nb + act[k];
     for (int k = ncols; k < 24; ++k) cols.col[k] = 0;
-    launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s);
+    launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s, c.gram_part_m);
     lob_small_eig(c, ncols, nb, drop, s);
     cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
     launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
@@ -672,7 +672,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (!use_best) cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
   if (launch_matvec(c, 0, true, X6, KX6, nb, nullptr, s)) return -2;
   if (launch_matvec(c, 1, true, X6, MX6, nb, nullptr, s)) return -2;
-  launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, GK, GM, s);
+  launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, GK, GM, s, c.gram_part_m);
   lob_small_eig(c, nb, nb, 1e-14, s);
   // X64 = X6 C (first nmodes columns)
   {

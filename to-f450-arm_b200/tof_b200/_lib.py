@@ -79,6 +79,7 @@ SIGNATURES = {
     "tof_mg_query": (c_int, [P, c_int, POINTER(c_int), POINTER(ctypes.c_float), P]),
     "tof_mg_export": (c_int, [P, c_int, P, P]),
     "tof_mg_apply": (c_int, [P, P, P, c_int, P]),
+    "tof_mg_setup": (c_int, [P, P]),
 }
 
 _lib = None

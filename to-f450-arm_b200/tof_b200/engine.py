@@ -201,6 +201,11 @@ class DesignContext:
         L.check("tof_mg_export", self.lib.tof_mg_export(self.h, level, L.ptr(out), _stream()), self.h)
         return out
 
+    def mg_setup(self):
+        """Build the multigrid hierarchy for the current density now, on the
+        current stream (before a static and a modal solve run concurrently)."""
+        L.check("tof_mg_setup", self.lib.tof_mg_setup(self.h, _stream()), self.h)
+
     def mg_apply(self, r4: torch.Tensor) -> torch.Tensor:
         r4 = r4.to(torch.float32).contiguous()
         e = torch.empty_like(r4)

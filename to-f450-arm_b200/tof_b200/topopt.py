@@ -11,6 +11,7 @@ host, as the reference's control flow needs them.
 """
 from __future__ import annotations
 
+import threading
 import time
 
 import numpy as np
@@ -58,6 +59,12 @@ class SIMPOptimizer:
 
     Extra keyword arguments (not in the reference):
       batch_loads  - solve all load cases as one block (default True);
+      concurrent   - in the mixed form, run the static solves and the modal
+                     solve of an iteration at the same time on two CUDA
+                     streams from two host threads (default True; each is a
+                     chain of short, latency-bound kernels that leaves most of
+                     the GPU idle, and the library keeps separate scratch for
+                     the two);
       solve_rtol   - static solve tolerance (default fem.SOLVE_RTOL);
       modal_tol    - LOBPCG relative residual tolerance (default 1e-5);
       x0_design    - start values on the design cells (reference order);
@@ -70,7 +77,8 @@ class SIMPOptimizer:
                  min_freq_Hz: float = None, tip_mass_kg: float = 0.060, n_modes_track: int = 4,
                  mu_freq_init: float = 0.10, mu_freq_max: float = 50.0, mu_freq_ramp_every: int = 5,
                  mu_freq_ramp_factor: float = 1.5, batch_loads: bool = True, solve_rtol: float = None,
-                 modal_tol: float = 1e-5, x0_design=None, F_list=None, modal_maxiter: int = None):
+                 modal_tol: float = 1e-5, x0_design=None, F_list=None, modal_maxiter: int = None,
+                 concurrent: bool = True):
         self.geom, self.fem = geom, fem
         self.load_cases = load_cases
         self.vol_frac = vol_frac
@@ -82,6 +90,8 @@ class SIMPOptimizer:
         self.mu_freq_ramp_every = max(1, int(mu_freq_ramp_every))
         self.mu_freq_ramp_factor = mu_freq_ramp_factor
         self.batch_loads = batch_loads
+        self.concurrent = concurrent
+        self._side = None                     # (static, modal) streams of the concurrent step
         self.solve_rtol = fem.SOLVE_RTOL if solve_rtol is None else solve_rtol
         self.modal_tol = modal_tol
         self.modal_maxiter = modal_maxiter
@@ -209,6 +219,30 @@ class SIMPOptimizer:
         self.history["modal_iters"].append(st["iters"])
         return modes, np.maximum(lam, 0.0)
 
+    def _static(self, mid):
+        """All load cases as one block (src/topopt.py:287-306), then the
+        weighted compliance and its filtered sensitivity (src/topopt.py:307-311).
+        Returns (filtered sensitivity, compliance as a device scalar)."""
+        ctx = self.ctx
+        R = self.b4.shape[0]
+        if self.batch_loads and mid == L.MODE_MIXED:
+            u4, st = ctx.pcg(self.b4, self.u4, rtol=self.solve_rtol, maxiter=20000, mode=mid)
+        else:
+            parts, st = [], []
+            for i in range(R):
+                ui, si = ctx.pcg(self.b4[i:i + 1], None if self.u4 is None else self.u4[i:i + 1],
+                                 rtol=self.solve_rtol, maxiter=20000, mode=mid)
+                parts.append(ui)
+                st += si
+            u4 = torch.cat(parts)
+        self.u4 = u4
+        self.stats.append(("pcg", st))
+        self.history["pcg_iters"].append(max(s["iters"] for s in st))
+        ce = ctx.quadform(L.OP_K, u4)
+        c_dev, dc = ctx.compliance_sens(ce, self.w_dev)
+        sens = self.filter.apply(dc, L.FILTER_FORWARD)       # src/topopt.py:311
+        return sens, c_dev
+
     def step(self):
         """One iteration of src/topopt.py:267-411; returns the change."""
         self.it += 1
@@ -224,32 +258,47 @@ class SIMPOptimizer:
             ctx.set_tip_lump(self._tip3)
             fem._tip_key = self._tip_key
         self._mark("filter+density")
-        # --- all load cases (src/topopt.py:287-306)
+        # --- all load cases (src/topopt.py:287-306) and the modes
+        # (src/topopt.py:313-330): independent given the density
         mid = fem._mode_id()
-        R = self.b4.shape[0]
-        if self.batch_loads and mid == L.MODE_MIXED:
-            u4, st = ctx.pcg(self.b4, self.u4, rtol=self.solve_rtol, maxiter=20000, mode=mid)
+        if self.concurrent and self.modal_active and mid == L.MODE_MIXED:
+            ctx.mg_setup()                                    # on the stream both sides wait on
+            main = torch.cuda.current_stream()
+            if self._side is None:
+                self._side = (torch.cuda.Stream(device=self.dev), torch.cuda.Stream(device=self.dev))
+            s_static, s_modal = self._side
+            s_static.wait_stream(main)
+            s_modal.wait_stream(main)
+            out = {}
+
+            def run(key, stream, fn):
+                try:
+                    with torch.cuda.stream(stream):
+                        out[key] = fn()
+                except BaseException as e:                    # re-raised below, after both joined
+                    out[key + "_error"] = e
+
+            t = threading.Thread(target=run, args=("static", s_static, lambda: self._static(mid)))
+            t.start()
+            run("modal", s_modal, lambda: self._modal(rho))
+            t.join()
+            main.wait_stream(s_static)
+            main.wait_stream(s_modal)
+            for key in ("static_error", "modal_error"):
+                if key in out:
+                    raise out[key]
+            sens, c_dev = out["static"]
+            modes, lam = out["modal"]
+            self._mark("static + modal solves")
         else:
-            parts, st = [], []
-            for i in range(R):
-                ui, si = ctx.pcg(self.b4[i:i + 1], None if self.u4 is None else self.u4[i:i + 1],
-                                 rtol=self.solve_rtol, maxiter=20000, mode=mid)
-                parts.append(ui)
-                st += si
-            u4 = torch.cat(parts)
-        self.u4 = u4
-        self.stats.append(("pcg", st))
-        self.history["pcg_iters"].append(max(s["iters"] for s in st))
-        self._mark("static solves")
-        ce = ctx.quadform(L.OP_K, u4)
-        c_dev, dc = ctx.compliance_sens(ce, self.w_dev)
-        sens = self.filter.apply(dc, L.FILTER_FORWARD)       # src/topopt.py:311
+            sens, c_dev = self._static(mid)
+            self._mark("static solves")
+            if self.modal_active:
+                modes, lam = self._modal(rho)
+                self._mark("modal solve")
         c_total = float(c_dev.item())
-        self._mark("compliance sens+filter")
         # --- modal constraint (src/topopt.py:313-375)
         if self.modal_active:
-            modes, lam = self._modal(rho)
-            self._mark("modal solve")
             if self.v_prev is None:
                 k = 0
             else:                                            # MAC, src/topopt.py:179-188
