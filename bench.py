@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip FP64/solver/CPU comparisons")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer and kernel-roofline runs "
                     "(profiling runs)")
+    ap.add_argument("--sequential-solves", action="store_true",
+                    help="issue the static and the modal solve of an iteration one after the other from one "
+                         "thread instead of concurrently (profiling runs; same work)")
     return ap.parse_args()
 
 
@@ -311,6 +314,7 @@ def own_arm(a, rank, world, local_rank):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     geom, fem, opt = arm_simp(mode="mixed")
+    opt.concurrent = not a.sequential_solves
     for _ in range(a.warmup):
         opt.step()
     torch.cuda.synchronize()
