@@ -261,6 +261,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.counters_m, 16)); A(dalloc(c, &c.status_m, 16)); A(dalloc(c, &c.scal_m, 256));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
   if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error);
+  mg_capture_all(c);
   A(cudaMemcpy(c.Ke64, Ke, 576 * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.Me64, Me, 576 * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.keb64, kb.data(), kb.size() * 8, cudaMemcpyHostToDevice));

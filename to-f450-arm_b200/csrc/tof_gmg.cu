@@ -960,35 +960,54 @@ static int vcycle_eager(Ctx& c, int R, int lane, cudaStream_t s) {
   return -1;
 }
 
+// Capture the V-cycle of one lane and R into a graph (recorded, not run).
+static bool capture_vcycle(Ctx& c, int lane, int ri, int R, cudaStream_t s) {
+  MG* mg = c.mg;
+  cudaGraphExec_t& ge = mg->vexec[lane][ri];
+  cudaGraph_t graph = nullptr;
+  bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  capturing() = ok;
+  if (ok) ok = vcycle_eager(c, R, lane, s) == 0;
+  capturing() = false;
+  const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
+  if (ok && ended && graph && cudaGraphInstantiate(&ge, graph, 0) == cudaSuccess) {
+    cudaGraphGetNodes(graph, nullptr, &mg->vnodes[lane][ri]);
+  } else {
+    ge = nullptr;
+    mg->vgraph_failed = true;
+  }
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
+  return ge != nullptr;
+}
+
+// All V-cycle graphs (both lanes, every R the context supports), recorded
+// once when the context is created: the buffers, tensor maps and smoothing
+// coefficients they reference never move, so no solve pays a capture and an
+// instantiation.
+int mg_capture_all(Ctx& c) {
+  MG* mg = c.mg;
+  cudaStream_t s = nullptr;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) { cudaGetLastError(); return 0; }
+  const int Rs[4] = {1, 2, 4, 8};
+  for (int lane = 0; lane < kLanes && !mg->vgraph_failed; ++lane)
+    for (int ri = 0; ri < 4 && !mg->vgraph_failed; ++ri)
+      if (Rs[ri] <= mg->maxR && !mg->vexec[lane][ri]) capture_vcycle(c, lane, ri, Rs[ri], s);
+  cudaStreamDestroy(s);
+  return 0;
+}
+
 // Apply the V-cycle to mg_rhs(c, lane) (R vectors); result in mg_out(c, lane).
 // Inside a stream capture (the PCG graphs) the kernels are recorded as they
-// are; otherwise the cycle for this lane and R is captured once and replayed
-// as a graph, which removes the per-kernel launch overhead of ~40 short
-// launches (the buffers, tensor maps and smoothing coefficients it references
-// never move).
+// are; otherwise the recorded graph of this lane and R is replayed, which
+// removes the per-kernel launch overhead of ~40 short launches.
 int mg_vcycle(Ctx& c, int R, cudaStream_t s, int lane) {
   MG* mg = c.mg;
   const int ri = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : -1;
   if (ri < 0 || lane < 0 || lane >= kLanes) return -1;
   if (capturing() || mg->vgraph_failed) return vcycle_eager(c, R, lane, s);
   cudaGraphExec_t& ge = mg->vexec[lane][ri];
-  if (!ge) {
-    cudaGraph_t graph = nullptr;
-    bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    capturing() = ok;
-    if (ok) ok = vcycle_eager(c, R, lane, s) == 0;
-    capturing() = false;
-    const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
-    if (ok && ended && graph && cudaGraphInstantiate(&ge, graph, 0) == cudaSuccess) {
-      cudaGraphGetNodes(graph, nullptr, &mg->vnodes[lane][ri]);
-    } else {
-      ge = nullptr;
-      mg->vgraph_failed = true;
-    }
-    if (graph) cudaGraphDestroy(graph);
-    cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
-    if (!ge) return vcycle_eager(c, R, lane, s);
-  }
+  if (!ge && !capture_vcycle(c, lane, ri, R, s)) return vcycle_eager(c, R, lane, s);
   if (cudaGraphLaunch(ge, s) != cudaSuccess) return -2;
   count_launch((long long)mg->vnodes[lane][ri]);
   return 0;

@@ -157,6 +157,7 @@ void mg_destroy(Ctx& c);
 int mg_setup(Ctx& c, cudaStream_t s);
 void mg_mark_dirty(Ctx& c);
 int mg_ensure(Ctx& c, cudaStream_t s);
+int mg_capture_all(Ctx& c);   // record every V-cycle graph once (context creation)
 int mg_vcycle(Ctx& c, int R, cudaStream_t s, int lane = 0);   // mg_rhs -> mg_out
 float* mg_rhs(Ctx& c, int lane = 0);
 float* mg_out(Ctx& c, int lane = 0);

@@ -470,6 +470,105 @@ __global__ void __launch_bounds__(kGramThreads) k_gram2_partial(int NN, const T*
   }
 }
 
+// FP64 inputs (LOBPCG's block vectors): the same tiling, with the staging of
+// chunk i + 1 overlapped with the products of chunk i.  A node4 FP64 record
+// (32 B, padding component 0) is copied unchanged into its row of the staging
+// buffer by two 16-byte cp.async operations, double-buffered in dynamic
+// shared memory; two CTAs per SM.
+constexpr size_t kGram2Smem = 2 * 72 * kGram2Ld * sizeof(double);
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(kGramThreads, 2) k_gram2_partial_f64(int NN, const double* __restrict__ A,
+                                                                       const double* __restrict__ B1,
+                                                                       const double* __restrict__ B2, ColMap cols,
+                                                                       int n, long long vstride, double* part) {
+  extern __shared__ __align__(16) double dsm[];     // [2][72 * kGram2Ld]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rg = lane & 7, cg = lane >> 3;
+  double acc1[3][6], acc2[3][6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) acc1[i][j] = acc2[i][j] = 0.0;
+  const int nchunks = (NN + kGram2Chunk - 1) / kGram2Chunk;
+  const int nstage = 3 * n * kGram2Chunk;
+  auto stage = [&](int ch, double* buf) {
+    const int n0 = ch * kGram2Chunk;
+    const int cnt = min(kGram2Chunk, NN - n0);
+    for (int idx = threadIdx.x; idx < nstage; idx += blockDim.x) {
+      const int v = idx / kGram2Chunk, q = idx % kGram2Chunk;
+      if (q >= cnt) continue;
+      const int blk = v / n, col = v % n;
+      const double* base = blk == 0 ? A : blk == 1 ? B1 : B2;
+      const double* src = base + cols.col[col] * vstride + 4 * (size_t)(n0 + q);
+      double* d = buf + (blk * 24 + col) * kGram2Ld + 4 * q;
+      cp_async16(d, src);
+      cp_async16(d + 2, src + 2);
+    }
+  };
+  int cur = 0;
+  if (blockIdx.x < nchunks) stage(blockIdx.x, dsm);
+  cp_async_commit();
+  for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int nx = ch + gridDim.x;
+    if (nx < nchunks) stage(nx, dsm + (cur ^ 1) * 72 * kGram2Ld);
+    cp_async_commit();
+    cp_async_wait<1>();                              // this chunk's copies are done
+    __syncthreads();
+    const double* sm = dsm + cur * 72 * kGram2Ld;
+    const int cnt = min(kGram2Chunk, NN - ch * kGram2Chunk);
+    const double* pa = sm + 3 * rg * kGram2Ld;
+    const double* pb1 = sm + (24 + 6 * cg) * kGram2Ld;
+    const double* pb2 = sm + (48 + 6 * cg) * kGram2Ld;
+    for (int q = w; q < cnt; q += kGramThreads / 32) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const int o = 4 * q + c;
+        double a[3], b1[6], b2[6];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) a[i] = pa[i * kGram2Ld + o];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) { b1[j] = pb1[j * kGram2Ld + o]; b2[j] = pb2[j * kGram2Ld + o]; }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 6; ++j) {
+            acc1[i][j] = fma(a[i], b1[j], acc1[i][j]);
+            acc2[i][j] = fma(a[i], b2[j], acc2[i][j]);
+          }
+      }
+    }
+    __syncthreads();                                 // the buffer is refilled two chunks later
+    cur ^= 1;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  double* red = dsm;                                   // [warp][576], one Gram at a time
+#pragma unroll
+  for (int g = 0; g < 2; ++g) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 6; ++j) red[w * 576 + (3 * rg + i) * 24 + 6 * cg + j] = g == 0 ? acc1[i][j] : acc2[i][j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, col = e % n;
+      double sum = 0.0;
+#pragma unroll
+      for (int k = 0; k < kGramThreads / 32; ++k) sum += red[k * 576 + r * 24 + col];
+      part[(size_t)blockIdx.x * 1152 + g * 576 + e] = sum;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256) k_gram2_reduce(int nblocks, int npair, const double* __restrict__ part,
                                                       double* G1, double* G2) {
   const int p = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -489,12 +588,16 @@ void launch_gram2_cols(Ctx& c, bool f64, const void* A, const void* B1, const vo
   int blocks = c.gram_blocks < nchunks ? c.gram_blocks : nchunks;
   if (blocks < 1) blocks = 1;
   const long long vs = (long long)c.g.NN * 4;
-  if (f64)
-    k_gram2_partial<double><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const double*)A, (const double*)B1,
-                                                           (const double*)B2, cols, n, vs, part);
-  else
+  if (f64) {
+    static_assert(2 * 72 * kGram2Ld >= 8 * 576, "reduction scratch");
+    cudaFuncSetAttribute(k_gram2_partial_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGram2Smem);
+    k_gram2_partial_f64<<<blocks, kGramThreads, kGram2Smem, s>>>(c.g.NN, (const double*)A, (const double*)B1,
+                                                                (const double*)B2, cols, n, vs, part);
+  }
+  else {
     k_gram2_partial<float><<<blocks, kGramThreads, 0, s>>>(c.g.NN, (const float*)A, (const float*)B1,
                                                           (const float*)B2, cols, n, vs, part);
+  }
   count_launch();
   k_gram2_reduce<<<ceil_div(2 * n * n, 8), 256, 0, s>>>(blocks, n * n, part, G1, G2);
   count_launch();

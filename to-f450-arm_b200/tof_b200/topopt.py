@@ -11,8 +11,8 @@ host, as the reference's control flow needs them.
 """
 from __future__ import annotations
 
-import threading
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -92,6 +92,7 @@ class SIMPOptimizer:
         self.batch_loads = batch_loads
         self.concurrent = concurrent
         self._side = None                     # (static, modal) streams of the concurrent step
+        self._worker = None                   # the host thread that issues the static solves
         self.solve_rtol = fem.SOLVE_RTOL if solve_rtol is None else solve_rtol
         self.modal_tol = modal_tol
         self.modal_maxiter = modal_maxiter
@@ -266,29 +267,30 @@ class SIMPOptimizer:
             main = torch.cuda.current_stream()
             if self._side is None:
                 self._side = (torch.cuda.Stream(device=self.dev), torch.cuda.Stream(device=self.dev))
+                self._worker = ThreadPoolExecutor(max_workers=1, thread_name_prefix="tof-static")
             s_static, s_modal = self._side
             s_static.wait_stream(main)
             s_modal.wait_stream(main)
-            out = {}
 
-            def run(key, stream, fn):
-                try:
-                    with torch.cuda.stream(stream):
-                        out[key] = fn()
-                except BaseException as e:                    # re-raised below, after both joined
-                    out[key + "_error"] = e
+            def static_side():
+                with torch.cuda.stream(s_static):
+                    return self._static(mid)
 
-            t = threading.Thread(target=run, args=("static", s_static, lambda: self._static(mid)))
-            t.start()
-            run("modal", s_modal, lambda: self._modal(rho))
-            t.join()
+            fut = self._worker.submit(static_side)
+            modal_exc = None
+            try:
+                with torch.cuda.stream(s_modal):
+                    modes, lam = self._modal(rho)
+            except BaseException as e:                        # raised after the static side joined
+                modal_exc = e
+            static_exc = fut.exception()
             main.wait_stream(s_static)
             main.wait_stream(s_modal)
-            for key in ("static_error", "modal_error"):
-                if key in out:
-                    raise out[key]
-            sens, c_dev = out["static"]
-            modes, lam = out["modal"]
+            if modal_exc is not None:
+                raise modal_exc
+            if static_exc is not None:
+                raise static_exc
+            sens, c_dev = fut.result()
             self._mark("static + modal solves")
         else:
             sens, c_dev = self._static(mid)
