@@ -273,8 +273,12 @@ class SIMPOptimizer:
             s_modal.wait_stream(main)
 
             def static_side():
+                # the worker waits for its own stream (free: the static side
+                # ends well before the modal side on these designs)
                 with torch.cuda.stream(s_static):
-                    return self._static(mid)
+                    out = self._static(mid)
+                s_static.synchronize()
+                return out
 
             fut = self._worker.submit(static_side)
             modal_exc = None
