@@ -9,6 +9,9 @@ voxels, 64 935 DOF): density filter, four load cases solved as one block
 1e-8), six lowest modes (FP64 LOBPCG with the FP32 multigrid preconditioner,
 eigenvalues converged to ~1e-10), MAC tracking, eigenvalue and compliance
 sensitivities, the augmented-Lagrangian frequency penalty and the OC update.
+The static and the modal solve of an iteration are issued concurrently on two
+streams (tof_b200.topopt.SIMPOptimizer, concurrent=True); --sequential-solves
+issues them from one thread (same work; for profilers).
 Inputs are synthetic (seeded) with the shapes of the reference's arm; see
 tof_b200/workloads.py.  With N GPUs every rank runs an independent replica
 (the path does not shard); value = N * K / max-rank time.
