@@ -79,7 +79,9 @@ int tof_version(void);
 /* Number of CUDA kernels this library has launched in the process (CUDA-graph
  * replays count their kernel nodes).  Diagnostics; no reference counterpart. */
 long long tof_launch_count(void);
-const char* tof_last_error(const tof_ctx* ctx);   /* ctx may be NULL: last create error */
+/* ctx may be NULL: the calling thread's last create error.  The string stays
+ * valid until the calling thread's next tof_last_error call. */
+const char* tof_last_error(const tof_ctx* ctx);
 
 /* Create a design context on the current CUDA device.
  * Replaces FEM3D.__init__ (src/fem.py:207-308): the element matrices are the

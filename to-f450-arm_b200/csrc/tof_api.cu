@@ -133,7 +133,10 @@ int tof_version(void) { return 100; }
 long long tof_launch_count(void) { return launch_counter().load(); }
 
 const char* tof_last_error(const tof_ctx* ctx) {
-  return ctx ? ctx->c.last_error.c_str() : g_create_error.c_str();
+  if (!ctx) return g_create_error.c_str();
+  static thread_local std::string copy;       // valid until this thread's next call
+  copy = ctx->c.last_error.str();
+  return copy.c_str();
 }
 
 int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[576], const double Me[576],
@@ -260,7 +263,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.gram_part_m, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.counters_m, 16)); A(dalloc(c, &c.status_m, 16)); A(dalloc(c, &c.scal_m, 256));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
-  if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error);
+  if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error.str());
   mg_capture_all(c);
   A(cudaMemcpy(c.Ke64, Ke, 576 * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.Me64, Me, 576 * 8, cudaMemcpyHostToDevice));

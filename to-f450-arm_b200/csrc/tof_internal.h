@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -38,6 +39,27 @@ struct SimpParams {
 // One design: grid, element matrices, boundary conditions, SIMP factors and
 // all solver workspace.  Everything is allocated in create(); solves never
 // allocate.
+// Error message of a context.  A static-family and a modal-family call may
+// run at the same time from two host threads, so the message is set and read
+// under a lock.
+class ErrorSlot {
+ public:
+  ErrorSlot& operator=(const std::string& m) {
+    std::lock_guard<std::mutex> g(mu_);
+    msg_ = m;
+    return *this;
+  }
+  ErrorSlot& operator=(const char* m) { return *this = std::string(m); }
+  std::string str() const {
+    std::lock_guard<std::mutex> g(mu_);
+    return msg_;
+  }
+
+ private:
+  mutable std::mutex mu_;
+  std::string msg_;
+};
+
 struct Ctx {
   int dev = 0;
   int num_sms = 0;
@@ -99,7 +121,7 @@ struct Ctx {
   MG* mg = nullptr;                // multigrid hierarchy (tof_gmg.cu)
   std::vector<uint8_t> host_fix;   // host copy of `fix`
   size_t bytes = 0;
-  std::string last_error;
+  ErrorSlot last_error;
 };
 
 // tensor-map encoding for a block of R node4 vectors (dtype float or double)
