@@ -40,3 +40,18 @@ def test_binding_load_sets_signatures():
     lib = L.load()
     assert lib.tof_ctx_create.restype is ctypes.c_int
     assert lib.tof_last_error(None) is not None or True
+
+
+def test_create_rejects_invalid_arguments_with_a_message():
+    """Argument errors are reported before any CUDA call, through
+    tof_last_error(NULL) (the calling thread's last create error)."""
+    from tof_b200 import _lib as L
+    lib = L.load()
+    h = ctypes.c_void_p()
+    Ke = (ctypes.c_double * 576)()
+    fixed = (ctypes.c_uint8 * 8)()
+    rc = lib.tof_ctx_create(0, 1, 1, None, Ke, Ke, None, fixed, None, None, 1, 1, None, ctypes.byref(h))
+    assert rc == L.TOF_ERR_ARG
+    msg = lib.tof_last_error(None)
+    msg = msg.decode() if isinstance(msg, bytes) else msg
+    assert "invalid argument" in msg
