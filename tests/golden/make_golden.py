@@ -292,11 +292,13 @@ def make_frf(rfem):
     return out
 
 
-def make_arm3d(with_modes=False):
+def make_arm3d(with_modes=False, default_material=False):
     """The reference's production domain (src/mesh3d.py ArmGeometry3D):
     masks, clamped nodes, tip-mass nodes and load vectors; with_modes: the
     lowest 6 exact FP64 frequencies of the solid domain with the 60 g tip
-    mass (src/fem.py:400-470 with the exact eigensolver)."""
+    mass (src/fem.py:400-470 with the exact eigensolver), for the PA12 of the
+    configs (rho 1010) or, with default_material, for the reference's default
+    Material() (src/fem.py:183-188, rho 930)."""
     from src.mesh3d import ArmGeometry3D
     g = ArmGeometry3D()
     m = g.build_masks()
@@ -310,7 +312,7 @@ def make_arm3d(with_modes=False):
     out["mz_dofs"], out["mz_vals"] = d, v
     if with_modes:
         import src.fem as rfem
-        fem = rfem.FEM3D(g, mat_ref(rfem))
+        fem = rfem.FEM3D(g, rfem.Material() if default_material else mat_ref(rfem))
         t0 = time.time()
         freqs, modes, lam = fem.modal_analysis(np.ones(fem.n_active), n_modes=6, tip_mass_kg=0.06)
         out = dict(freqs=freqs, lam=lam, n_free=len(fem.free_dofs), seconds=time.time() - t0)
@@ -332,6 +334,10 @@ def main():
         return
     if a.only == "arm3d_modes":
         np.savez_compressed(os.path.join(HERE, "arm3d_modes.npz"), **make_arm3d(with_modes=True))
+        return
+    if a.only == "arm3d_modes_930":
+        np.savez_compressed(os.path.join(HERE, "arm3d_modes_930.npz"),
+                            **make_arm3d(with_modes=True, default_material=True))
         return
     if a.only == "frf":
         np.savez_compressed(os.path.join(HERE, "frf.npz"), **make_frf(rfem))

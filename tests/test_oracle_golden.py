@@ -181,3 +181,20 @@ def test_oracle_frf(golden):
         np.testing.assert_allclose(H, d[f"H{i}"], rtol=1e-13)
     f, H = modal_frf_at_dof(d["freqs"], d["modes"], int(d["dofs"][0]), (50.0, 4000.0), 257, 0.05)
     np.testing.assert_allclose(H, d["H_alt"], rtol=1e-13)
+
+
+def test_production_domain_default_material_known_answer(golden):
+    """The fixture generator's exact FP64 eigensolve of the reference's
+    production domain (ArmGeometry3D, solid, 60 g tip mass, 198 093 free DOF)
+    with the reference's default Material() (rho 930 kg/m^3) gives the known
+    exact frequencies of that domain, 203.891, 247.267, 801.087, 1234.547,
+    1249.151 and 1636.433 Hz.  arm3d_modes.npz, which the production-domain
+    GPU test uses, is the same computation for the PA12 of the configs
+    (rho 1010), hence its lower frequencies."""
+    g = golden("arm3d_modes_930")
+    known = np.array([203.891, 247.267, 801.087, 1234.547, 1249.151, 1636.433])
+    assert int(g["n_free"]) == 198093
+    assert np.allclose(np.round(g["freqs"], 3), known, rtol=0, atol=1e-9)
+    g1010 = golden("arm3d_modes")
+    assert int(g1010["n_free"]) == 198093
+    assert np.all(g1010["freqs"] < g["freqs"])
