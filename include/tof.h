@@ -66,6 +66,10 @@ typedef struct {
   int outer;      /* refinement steps (mixed PCG), else 1 */
   double relres;  /* PCG: ||b - K x||_2 / ||b||_2 recomputed in FP64 at exit.
                      LOBPCG: largest ||K x - theta M x|| / ||K x|| of the modes */
+  double floor;   /* PCG: FP64 rounding floor of relres, eps ||(|K||x| + |b|)|| / ||b||
+                     (what rounding the exact solution to FP64 can leave); the
+                     solve counts as converged when relres <= max(rtol, floor).
+                     LOBPCG: 0 */
 } tof_solve_stats;
 
 /* SIMP interpolation constants: stiffness emin + (1-emin) rho^penal,
@@ -108,6 +112,19 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
                    const tof_simp_params* simp, int max_rhs, int max_modes, const int tile[3], tof_ctx** out);
 void tof_ctx_destroy(tof_ctx* ctx);
 long long tof_ctx_query(const tof_ctx* ctx, int what);
+/* Wait budget of the context's persistent solver kernels (ns, 1 us .. 60 s;
+ * default 2 s).  Every device-side wait of those kernels (grid barriers,
+ * TMA tile arrivals) gives up after it: the solve then returns
+ * TOF_ERR_TIMEOUT and the context stays usable.  No reference counterpart:
+ * the reference's solvers run on the host and signal failure by `info != 0`
+ * and a fallback solver (src/fem.py:548-550, src/fem_gpu.py:84-91). */
+int tof_ctx_set_wait_limit(tof_ctx* ctx, long long ns);
+/* Exercises that bounded wait: a few CTAs meet at one grid barrier that
+ * expects `extra_arrivals` (0 or 1) more arrivals than the launch has.  With
+ * 0 the barrier completes (TOF_OK); with 1 nobody releases it, every CTA
+ * gives up after the wait budget and the call returns TOF_ERR_TIMEOUT.  The
+ * barrier is reset either way.  Diagnostics; no reference counterpart. */
+int tof_wait_selftest(tof_ctx* ctx, int extra_arrivals, void* stream);
 
 /* Set element densities (device FP64 [NE]); computes SIMP stiffness and mass
  * factors and the diagonals.  Replaces the per-call assemble_K / assemble_M
@@ -136,7 +153,10 @@ int tof_diag(tof_ctx* ctx, int op, double* out, void* stream);
  * vectors on entry and the solution on exit.  Replaces
  * FEM3D.apply_BCs_and_solve / FEM3D.solve (src/fem.py:529-561) and the GPU
  * drop-in _solve_cg_gpu (src/fem_gpu.py:46-98); stops at
- * ||b - K x||_2 <= rtol ||b||_2 like SciPy's cg.  Synchronises `stream`;
+ * ||b - K x||_2 <= rtol ||b||_2 like SciPy's cg, the residual recomputed in
+ * FP64 at exit; where FP64 cannot represent a solution that good (the
+ * rounding floor in tof_solve_stats.floor is above rtol) a true residual at
+ * that floor counts as converged.  Synchronises `stream`;
  * stats (host, nrhs entries) may be NULL. */
 int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double rtol, int maxiter,
             tof_solve_stats* stats, void* stream);
@@ -162,8 +182,9 @@ int tof_mg_setup(tof_ctx* ctx, void* stream);
  * M-orthonormal modes, ascending, in its first nmodes vectors on exit;
  * lam (host, nmodes) gets the eigenvalues (rad/s)^2.  Replaces
  * FEM3D.modal_analysis (src/fem.py:400-470) and _modal_gpu
- * (src/fem_gpu.py:101-173).  precond: TOF_PRECOND_JACOBI (as the reference)
- * or TOF_PRECOND_PCG (inner_iters pipelined PCG iterations to inner_rtol).
+ * (src/fem_gpu.py:101-173).  precond: TOF_PRECOND_JACOBI (as the reference),
+ * TOF_PRECOND_PCG (inner_iters FP32 PCG iterations to inner_rtol) or
+ * TOF_PRECOND_MG (inner_iters FP32 multigrid V-cycles, at least one).
  * Synchronises `stream`.  resid (host, nmodes) may be NULL. */
 int tof_lobpcg(tof_ctx* ctx, int mode, int nmodes, int block, double* X, double* lam, double tol, int maxiter,
                int precond, int inner_iters, double inner_rtol, tof_solve_stats* stats, double* resid,
@@ -181,17 +202,18 @@ int tof_gram(tof_ctx* ctx, int dtype, const void* A, int na, const void* B, int 
 /* The same G = A^T B without a context and without allocating any device
  * memory; no counterpart in the reference.  For callers that cannot allocate
  * device memory when they need it: a host application whose memory pool owns
- * the whole GPU, code issuing work while a stream is being captured into a
- * CUDA graph (where cudaMalloc is not allowed), or a loop that must not take
+ * the whole GPU and refuses other allocations, or a loop that must not take
  * cudaMalloc's implicit device synchronisation.  A, B: node4 blocks of
  * n_nodes nodes, dtype TOF_F32 or TOF_F64; G: device FP64 na x nb.
- * Limits: na, nb <= 24 and n_nodes < 2^31, else TOF_ERR_ARG with a message in
- * tof_last_error(NULL).  Temporaries live in one fixed device array of about
- * 1.1 MiB that every GPU loading the library keeps until the process exits;
- * the first call on a device looks up that array's device address (issue it
- * before any stream capture).  All calls on a GPU share the array and it
- * keeps the previous call's contents: calls whose executions overlap on the
- * same GPU race, so order them (one stream, or events). */
+ * Limits: na, nb <= 24 and n_nodes <= INT_MAX, else TOF_ERR_ARG with a
+ * message in tof_last_error(NULL).  Temporaries live in one fixed device
+ * array of about 1.1 MiB that is part of this library's device code: it takes
+ * its device memory at the first call on each device (CUDA loads device code
+ * lazily) and keeps it until the process exits.  That first call also looks
+ * up the array's device address, so make it before any stream capture and
+ * before a memory pool takes over the GPU.  All calls on a GPU share the
+ * array and it keeps the previous call's contents: calls whose executions
+ * overlap on the same GPU race, so order them (one stream, or events). */
 int tof_gram_noalloc(long long n_nodes, int dtype, const void* A, int na, const void* B, int nb, double* G,
                      void* stream);
 

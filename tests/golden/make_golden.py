@@ -1,8 +1,9 @@
 """Generate golden fixtures by running the reference solver itself.
 
-Run in a container that has the reference source tree (read-only):
+Run in a container that has the reference source tree (read-only), passing
+its root directory:
 
-    python tests/golden/make_golden.py --ref /root/reference [--skip-arm] [--only stress|frf|arm3d|arm3d_modes]
+    python tests/golden/make_golden.py --ref <reference checkout> [--skip-arm] [--only stress|frf|arm3d|arm3d_modes]
 
 The reference (NinhGhoster/TO-F450-arm, pure Python + SciPy) is imported from
 its own `src/` and `sims/` packages and driven with the synthetic geometries of
@@ -319,11 +320,140 @@ def make_arm3d(with_modes=False, default_material=False):
     return out
 
 
+def make_arm_c3(rfem, rtop, rmp, n_iter=50):
+    """The differentiation / SIMP workload on the 2 mm arm grid, run by the
+    reference's own SIMPOptimizer.run (src/topopt.py:217-427) with exact
+    solves: start design vf 0.08 + U(-0.02, 0.02) (seed 0), filter radius
+    3 mm, 500 Hz augmented-Lagrangian target with mu 0.2, 6 tracked modes,
+    60 g tip mass, four load cases (thrust; torque about the arm axis plus
+    lateral; both; 3 g inertial from the reference's assembled M at the start
+    design).  Records the first iteration's physical density, per-load-case
+    compliances, frequencies and effective masses (6 and 8 modes), the
+    sensitivity handed to the OC update in iterations 1 and 2, and the
+    history of all n_iter iterations.
+
+    The inputs (geometry, start values, surface loads) come from
+    tof_b200.configs; the start values enter through the one place the
+    reference reads vol_frac for them (src/topopt.py:231, an element-wise
+    np.where), after target_volume has been computed from the scalar."""
+    from scipy.sparse.linalg import splu
+    g = C.arm_geometry()
+    fem = rfem.FEM3D(g, mat_ref(rfem))
+    masks = g.build_masks()
+    x0 = C.arm_design_start(g, vf=0.08, seed=0).astype(np.float64)
+    fr = fem.free_dofs
+    lu_cache = {}
+
+    def factor(Kff):
+        """One sparse LU of K_ff per density, shared by the four static
+        solves and the shift-invert eigensolve of that iteration."""
+        key = hash(Kff.data.tobytes())
+        if key not in lu_cache:
+            lu_cache.clear()
+            lu_cache[key] = splu(Kff, permc_spec="MMD_AT_PLUS_A")
+        return lu_cache[key]
+
+    def lu_solve(self, K, F, method="cg", x0=None, rtol=1e-5):
+        u = np.zeros(self.geom.n_dofs)
+        u[fr] = factor(K[fr][:, fr].tocsc()).solve(F[fr])
+        return u
+
+    def eigs_shared_lu(K, X, B=None, M=None, tol=None, largest=False, maxiter=None, **kw):
+        lu = factor(K.tocsc())
+        op = spla.LinearOperator(K.shape, matvec=lu.solve, dtype=np.float64)
+        return spla.eigsh(K, k=X.shape[1], M=B.tocsc(), sigma=0.0, which="LM", tol=1e-13, maxiter=50000,
+                          OPinv=op)
+
+    rec = dict(solves=[], modal=[], dc=[], x=[], xs=[])
+    orig_solve = rfem.FEM3D.apply_BCs_and_solve
+    orig_solve_fn = rfem.FEM3D.solve
+    orig_modal = rfem.FEM3D.modal_analysis
+    orig_oc = rtop.SIMPOptimizer._oc_update
+
+    def solve(self, rho_active, F, method="cg", x0=None):
+        u = orig_solve_fn(self, rho_active, F, method, x0)
+        if len(rec["solves"]) < 4:
+            rec["solves"].append((rho_active.copy(), u.copy()))
+        return u
+
+    def modal(self, rho_active, *a, **kw):
+        out = orig_modal(self, rho_active, *a, **kw)
+        if not rec["modal"]:
+            rec["modal"].append(out)
+        return out
+
+    def oc(self, x, dc):
+        print(f"  arm_c3 iteration {len(rec['x']) + 1}: {time.time() - t0:.0f}s", flush=True)
+        rec["x"].append(None)
+        if len(rec["dc"]) < 2:
+            rec["dc"].append(dc.copy())
+            rec["xs"].append(x.copy())
+        return orig_oc(self, x, dc)
+
+    orig_lobpcg = rfem.spla.lobpcg
+    rfem.spla.lobpcg = eigs_shared_lu
+    rfem.FEM3D.apply_BCs_and_solve = lu_solve
+    rfem.FEM3D.solve = solve
+    rfem.FEM3D.modal_analysis = modal
+    rtop.SIMPOptimizer._oc_update = oc
+    t0 = time.time()
+    try:
+        F3 = C.arm_static_loads(g)
+        opt = rtop.SIMPOptimizer(g, fem, load_cases=[dict(F=(0, 0, 0))] * 4, vol_frac=0.08, r_min_mm=3.0,
+                                 move=0.2, max_iter=n_iter, tol_change=0.0, min_freq_Hz=500.0,
+                                 tip_mass_kg=C.TIP_MASS_KG, n_modes_track=6, mu_freq_init=0.2,
+                                 mu_freq_max=50.0, mu_freq_ramp_every=5, mu_freq_ramp_factor=1.5)
+        # start values on the design cells (reference design-cell order)
+        grid = np.zeros((g.nx, g.ny, g.nz))
+        grid[masks["design"]] = x0
+        ex, ey, ez = fem.elem_grid_idx.T
+        v0 = np.ones(fem.n_active)
+        dsg = opt.is_design_active
+        v0[dsg] = grid[ex, ey, ez][dsg]
+        # start physical density as run() forms it, for the inertial load
+        rg = np.zeros((g.nx, g.ny, g.nz))
+        rg[ex, ey, ez] = np.where(dsg, v0, 1.0)
+        ph = rtop.filter_field(rg, opt.design_mask_grid, opt.kernel)
+        ph[~opt.design_mask_grid] = 0.0
+        ph = np.where(opt.design, ph, np.where(opt.in_arm, 1.0, 0.0))
+        rho_start = ph[ex, ey, ez]
+        ez_vec = np.zeros(g.n_dofs)
+        ez_vec[2::3] = 1.0
+        Mr = fem.assemble_M(rho_start, C.TIP_MASS_KG, g.motor_mount_top_nodes()) @ ez_vec
+        F_list = F3 + [C.body_load_from_Mr(Mr, 3.0)]
+        opt.F_list = [f.copy() for f in F_list]
+        opt.vol_frac = v0
+        res = opt.run(verbose=False)
+        t_run = time.time() - t0
+        freqs8, modes8, lam8 = rfem.FEM3D.modal_analysis(fem, rec["solves"][0][0], n_modes=8,
+                                                         tip_mass_kg=C.TIP_MASS_KG)
+    finally:
+        rfem.spla.lobpcg = orig_lobpcg
+        rfem.FEM3D.apply_BCs_and_solve = orig_solve
+        rfem.FEM3D.solve = orig_solve_fn
+        rfem.FEM3D.modal_analysis = orig_modal
+        rtop.SIMPOptimizer._oc_update = orig_oc
+    rho1 = rec["solves"][0][0]
+    comp1 = np.array([float(F @ u) for F, (_, u) in zip(F_list, rec["solves"])])
+    freqs1, modes1, lam1 = rec["modal"][0]
+    eff1 = rmp.effective_mass_voxel(fem, g, rho1, modes1, C.TIP_MASS_KG, direction=2)
+    eff8 = rmp.effective_mass_voxel(fem, g, rho1, modes8, C.TIP_MASS_KG, direction=2)
+    h = res["history"]
+    print(f"arm_c3: {n_iter} iterations in {t_run:.0f}s; c {h['compliance'][0]:.6e} -> {h['compliance'][-1]:.6e}")
+    return dict(x0=x0, F=np.stack(F_list), rho1=rho1, compliance_lc1=comp1, freqs1=freqs1, lam1=lam1, eff1=eff1,
+                freqs8=freqs8, lam8=lam8, eff8=eff8, dc1=rec["dc"][0], dc2=rec["dc"][1], x2=rec["xs"][1],
+                compliance=np.array(h["compliance"]), change=np.array(h["change"]),
+                vf_hist=np.array(h["vol_frac"]), omega1=np.array(h["omega_1_Hz"]),
+                mu_hist=np.array(h["mu_freq"]), viol=np.array(h["freq_violation"]),
+                rho_final=res["rho_active"], n_iter=n_iter, seconds=t_run)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference checkout (holds src/ and sims/)")
     ap.add_argument("--skip-arm", action="store_true")
     ap.add_argument("--only", default=None, help="write just this fixture (e.g. stress)")
+    ap.add_argument("--iters", type=int, default=50, help="SIMP iterations of the arm_c3 fixture")
     a = ap.parse_args()
     rfem, rtop, rmp = setup_reference(a.ref)
     if a.only == "stress":
@@ -338,6 +468,9 @@ def main():
     if a.only == "arm3d_modes_930":
         np.savez_compressed(os.path.join(HERE, "arm3d_modes_930.npz"),
                             **make_arm3d(with_modes=True, default_material=True))
+        return
+    if a.only == "arm_c3":
+        np.savez_compressed(os.path.join(HERE, "arm_c3.npz"), **make_arm_c3(rfem, rtop, rmp, n_iter=a.iters))
         return
     if a.only == "frf":
         np.savez_compressed(os.path.join(HERE, "frf.npz"), **make_frf(rfem))

@@ -1,5 +1,6 @@
 // C ABI of libtof: context management and the reference-facing entry points.
 #include <math.h>
+#include <stddef.h>
 #include <string.h>
 
 #include <algorithm>
@@ -118,7 +119,7 @@ static cudaError_t dalloc(Ctx& c, T** p, size_t n) {
 
 static void free_ctx(Ctx& c) {
   mg_destroy(c);
-  void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
+  void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.kebabs64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
                   c.fK64, c.fM64, c.fK32, c.fM32, c.rho, c.dK64, c.dM64, c.dinvK64, c.dinvK32, c.partials,
                   c.bar, c.status, c.scal, c.counters, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part,
                   c.gram_part_m, c.counters_m, c.status_m, c.scal_m};
@@ -245,6 +246,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
   A(dalloc(c, &c.Ke64, 576)); A(dalloc(c, &c.Me64, 576));
   A(dalloc(c, &c.keb64, kKeBlocksLen)); A(dalloc(c, &c.meb64, kKeBlocksLen));
+  A(dalloc(c, &c.kebabs64, kKeBlocksLen));
   A(dalloc(c, &c.keb32, kKeBlocksLen)); A(dalloc(c, &c.meb32, kKeBlocksLen));
   A(dalloc(c, &c.active, NE)); A(dalloc(c, &c.fix, NN));
   A(dalloc(c, &c.tip64, V)); A(dalloc(c, &c.tip32, V));
@@ -269,6 +271,11 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(cudaMemcpy(c.Me64, Me, 576 * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.keb64, kb.data(), kb.size() * 8, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.meb64, mb.data(), mb.size() * 8, cudaMemcpyHostToDevice));
+  {
+    std::vector<double> kabs(kb.size());
+    for (size_t q = 0; q < kb.size(); ++q) kabs[q] = fabs(kb[q]);
+    A(cudaMemcpy(c.kebabs64, kabs.data(), kabs.size() * 8, cudaMemcpyHostToDevice));
+  }
   A(cudaMemcpy(c.keb32, kbf.data(), kbf.size() * 4, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.meb32, mbf.data(), mbf.size() * 4, cudaMemcpyHostToDevice));
   A(cudaMemcpy(c.active, act.data(), NE, cudaMemcpyHostToDevice));
@@ -294,6 +301,41 @@ void tof_ctx_destroy(tof_ctx* ctx) {
   cudaDeviceSynchronize();
   free_ctx(ctx->c);
   delete ctx;
+}
+
+int tof_ctx_set_wait_limit(tof_ctx* ctx, long long ns) {
+  if (!ctx) return TOF_ERR_ARG;
+  Ctx& c = ctx->c;
+  if (ns < 1000 || ns > 60000000000LL) {
+    c.last_error = "tof_ctx_set_wait_limit: the limit must be in [1 us, 60 s]";
+    return TOF_ERR_ARG;
+  }
+  const unsigned long long w = (unsigned long long)ns;
+  CUDA_TRY(cudaMemcpy(reinterpret_cast<char*>(c.bar) + offsetof(BarrierState, wait_ns), &w, sizeof(w),
+                      cudaMemcpyHostToDevice));
+  c.wait_ns = ns;
+  return TOF_OK;
+}
+
+int tof_wait_selftest(tof_ctx* ctx, int extra_arrivals, void* stream) {
+  if (!ctx || extra_arrivals < 0 || extra_arrivals > 1) return TOF_ERR_ARG;
+  Ctx& c = ctx->c;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int G = std::min(4, std::max(1, c.num_sms));
+  CUDA_TRY(cudaMemsetAsync(c.bar, 0, kBarrierResetBytes, s));
+  if (launch_barrier_selftest(c, G, G + extra_arrivals, s)) return TOF_ERR_CUDA;
+  int err = 0;
+  CUDA_TRY(cudaMemcpyAsync(&err, reinterpret_cast<char*>(c.bar) + offsetof(BarrierState, error), sizeof(int),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  // leave the barrier ready for the next persistent launch
+  CUDA_TRY(cudaMemsetAsync(c.bar, 0, kBarrierResetBytes, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (err == ST_TIMEOUT) {
+    c.last_error = "tof_wait_selftest: grid barrier wait budget expired";
+    return TOF_ERR_TIMEOUT;
+  }
+  return err ? TOF_ERR_CUDA : TOF_OK;
 }
 
 long long tof_ctx_query(const tof_ctx* ctx, int what) {
@@ -389,19 +431,39 @@ int tof_gram(tof_ctx* ctx, int dtype, const void* A, int na, const void* B, int 
 // ---------------------------------------------------------------------------
 // PCG
 // ---------------------------------------------------------------------------
-static int true_relres(Ctx& c, const double* b, const double* x, int R, double* rel, cudaStream_t s) {
-  const size_t blk = (size_t)c.max_rhs * c.g.NN * 4;
+// rel[k] = ||b_k - K x_k|| / ||b_k|| recomputed in FP64, and the rounding
+// floor of that residual, phi[k] = eps ||(|K| |x_k| + |b_k|)|| / ||b_k||:
+// rounding the exact solution to FP64 alone leaves a residual up to
+// eps |K| |x| (componentwise), so a true residual at or below phi is as
+// small as FP64 can represent.  On soft SIMP designs |K||x| / |b| reaches
+// 1e8, which puts phi above 1e-8 (a sparse LU solution then shows the same
+// true residual).  Uses FP64 work slots 4, 5 and 7.
+static int true_relres(Ctx& c, const double* b, const double* x, int R, double* rel, cudaStream_t s,
+                       double* phi = nullptr) {
+  const size_t V = (size_t)c.g.NN * 4;
+  const size_t blk = (size_t)c.max_rhs * V;
   double* r64 = c.pw64 + 7 * blk;
   if (launch_matvec(c, 0, true, x, r64, R, b, s)) return TOF_ERR_CUDA;
   launch_gram(c, true, r64, R, r64, R, c.gram + 4 * 576, s);
   launch_gram(c, true, b, R, b, R, c.gram + 5 * 576, s);
-  double G[2][64];
+  if (phi) {
+    double* ax = c.pw64 + 5 * blk;
+    double* y = c.pw64 + 4 * blk;
+    launch_abs64((long long)R * V, x, ax, s);
+    if (launch_matvec(c, 2, true, ax, y, R, nullptr, s)) return TOF_ERR_CUDA;
+    launch_abs64((long long)R * V, b, ax, s);
+    launch_axpy64((long long)R * V, ax, y, 1.0, s);
+    launch_gram(c, true, y, R, y, R, c.gram + 7 * 576, s);
+  }
+  double G[3][64];
   CUDA_TRY(cudaMemcpyAsync(G[0], c.gram + 4 * 576, sizeof(double) * R * R, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaMemcpyAsync(G[1], c.gram + 5 * 576, sizeof(double) * R * R, cudaMemcpyDeviceToHost, s));
+  if (phi) CUDA_TRY(cudaMemcpyAsync(G[2], c.gram + 7 * 576, sizeof(double) * R * R, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   for (int k = 0; k < R; ++k) {
     const double bn = sqrt(G[1][k * R + k]);
     rel[k] = bn > 0.0 ? sqrt(G[0][k * R + k]) / bn : 0.0;
+    if (phi) phi[k] = bn > 0.0 ? 2.220446049250313e-16 * sqrt(G[2][k * R + k]) / bn : 0.0;
   }
   return TOF_OK;
 }
@@ -423,18 +485,32 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
   CUDA_TRY(cudaMemcpyAsync(wx, x, sizeof(double) * nrhs * V, cudaMemcpyDeviceToDevice, s));
   int st[16] = {0};
   double rel[8] = {0};
+  double phi[8] = {0};
   int iters[8] = {0}, outer[8] = {0};
   int rc = TOF_OK;
   if (mode == TOF_MODE_FP64) {
-    if (pcg_plain64(c, wb, wx, R, rtol, maxiter, nullptr, nullptr, nullptr, s)) return TOF_ERR_CUDA;
-    CUDA_TRY(cudaMemcpyAsync(st, c.status, sizeof(int) * 2 * R, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    for (int k = 0; k < nrhs; ++k) { iters[k] = st[R + k]; outer[k] = 1; }
-    if (true_relres(c, wb, wx, R, rel, s)) return TOF_ERR_CUDA;
-    for (int k = 0; k < nrhs; ++k) {
-      int sk = st[k];
-      if (sk == ST_OK && rel[k] > rtol * 1.01) sk = ST_NOT_CONVERGED;
-      st[k] = sk;
+    // SciPy's recurrence; when its recursive residual claims rtol but the
+    // true residual (recomputed in FP64) exceeds max(rtol, rounding floor),
+    // the iteration restarts from the current x (residual replacement), at
+    // most kMaxRestarts times.  Right-hand sides already done restart from
+    // their converged x and stop at once.
+    constexpr int kMaxRestarts = 4;
+    for (int o = 0; o <= kMaxRestarts; ++o) {
+      const int budget = maxiter - *std::max_element(iters, iters + nrhs);
+      if (budget <= 0) break;
+      if (pcg_plain64(c, wb, wx, R, rtol, budget, nullptr, nullptr, nullptr, s)) return TOF_ERR_CUDA;
+      int sto[16] = {0};
+      CUDA_TRY(cudaMemcpyAsync(sto, c.status, sizeof(int) * 2 * R, cudaMemcpyDeviceToHost, s));
+      CUDA_TRY(cudaStreamSynchronize(s));
+      if (true_relres(c, wb, wx, R, rel, s, phi)) return TOF_ERR_CUDA;
+      bool again = false;
+      for (int k = 0; k < nrhs; ++k) {
+        iters[k] += sto[R + k];
+        outer[k] = o + 1;
+        st[k] = sto[k];
+        if (st[k] == ST_OK && rel[k] > std::max(rtol, phi[k]) * 1.01) { st[k] = ST_NOT_CONVERGED; again = true; }
+      }
+      if (!again) break;
     }
   } else if (mode == TOF_MODE_MIXED) {
     // FP64 PCG preconditioned by the FP32 multigrid V-cycle.  The recursive
@@ -449,13 +525,13 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       const int budget = maxiter - *std::max_element(iters, iters + R);
       if (budget <= 0) break;
       if (pcg_mg64(c, wb, wx, R, rtol, budget, it_o, ist, s)) return TOF_ERR_CUDA;
-      if (true_relres(c, wb, wx, R, rel, s)) return TOF_ERR_CUDA;
+      if (true_relres(c, wb, wx, R, rel, s, phi)) return TOF_ERR_CUDA;
       bool again = false;
       for (int k = 0; k < nrhs; ++k) {
         iters[k] += it_o[k];
         outer[k] = o + 1;
         st[k] = ist[k];
-        if (st[k] == ST_OK && rel[k] > rtol * 1.01) { st[k] = ST_NOT_CONVERGED; again = true; }
+        if (st[k] == ST_OK && rel[k] > std::max(rtol, phi[k]) * 1.01) { st[k] = ST_NOT_CONVERGED; again = true; }
       }
       if (!again) break;
     }
@@ -520,6 +596,7 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       stats[k].iters = iters[k];
       stats[k].outer = outer[k];
       stats[k].relres = rel[k];
+      stats[k].floor = phi[k];
     }
   }
   return rc;
@@ -573,6 +650,7 @@ int tof_lobpcg(tof_ctx* ctx, int mode, int nmodes, int block, double* X, double*
     double w = 0.0;
     for (int j = 0; j < nmodes; ++j) w = std::max(w, res[j]);
     stats->relres = w;
+    stats->floor = 0.0;
   }
   if (rc == -2) return TOF_ERR_CUDA;
   return rc;

@@ -86,7 +86,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 
 // Wait budget of every spin in this library: a wait that has not completed
 // after this long gives up, raises an error flag and returns (a legitimate
-// wait here lasts microseconds).
+// wait here lasts microseconds).  Persistent solver kernels take the budget
+// of their context (BarrierState::wait_ns, tof_ctx_set_wait_limit); 0 means
+// this default.
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;   // 2 s
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -107,7 +109,15 @@ struct BarrierState {
   unsigned gen;
   int error;   // nonzero: some CTA gave up; everybody leaves
   int pad;
+  unsigned long long wait_ns;   // wait budget (0: kWaitLimitNs); kept across resets
 };
+// bytes of BarrierState cleared before each persistent launch (wait_ns stays)
+constexpr size_t kBarrierResetBytes = 16;
+
+__device__ __forceinline__ unsigned long long wait_budget(const BarrierState* bs) {
+  const unsigned long long w = bs->wait_ns;
+  return w ? w : kWaitLimitNs;
+}
 
 __device__ __forceinline__ bool grid_barrier(BarrierState* bs, unsigned nblocks) {
   __shared__ int s_ok;
@@ -125,9 +135,10 @@ __device__ __forceinline__ bool grid_barrier(BarrierState* bs, unsigned nblocks)
     } else {
       unsigned long long spins = 0;
       const unsigned long long t0 = global_ns();
+      const unsigned long long limit = wait_budget(bs);
       while (ld_acquire_u32(&bs->gen) == g) {
         if (ld_relaxed_i32(&bs->error)) { ok = 0; break; }
-        if ((++spins & 255) == 0 && global_ns() - t0 > kWaitLimitNs) {
+        if ((++spins & 255) == 0 && global_ns() - t0 > limit) {
           atomicExch(&bs->error, ST_TIMEOUT);
           ok = 0;
           break;
@@ -154,12 +165,13 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
 }
-// Bounded wait on phase `parity`; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Bounded wait on phase `parity`; returns false after `limit` ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned long long limit = kWaitLimitNs) {
   uint32_t addr = smem_u32(bar);
   const unsigned long long t0 = global_ns();
   for (unsigned long long i = 0;; ++i) {
-    if ((i & 1023) == 1023 && global_ns() - t0 > kWaitLimitNs) return false;
+    if ((i & 1023) == 1023 && global_ns() - t0 > limit) return false;
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"

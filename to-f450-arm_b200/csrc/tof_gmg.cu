@@ -1063,7 +1063,7 @@ int mg_levels(const Ctx& c) { return c.mg ? c.mg->nlev : 0; }
 // FP64 PCG preconditioned by the FP32 V-cycle
 // ---------------------------------------------------------------------------
 // scalar layout per rhs k: S[k*8 + {0: rz, 1: alpha, 2: beta, 3: rr, 4: bnorm, 5: iters}]
-// flags[k]: 0 active, 1 converged, 2 breakdown / non-finite
+// flags[k]: 0 active, 1 converged, 2 breakdown (p.q <= 0), 3 non-finite
 
 // r = b - A x0 already computed into mg->r; r32 = (float) r; rr, bb
 template <int R>
@@ -1096,7 +1096,7 @@ __global__ void __launch_bounds__(256) k_mgpcg_init(int NN, const double* __rest
       S[k * 8 + 5] = 0.0;
       S[k * 8 + 2] = 0.0;
       int f = 0;
-      if (!isfinite(tot[2 * k]) || !isfinite(bn)) f = 2;
+      if (!isfinite(tot[2 * k]) || !isfinite(bn)) f = 3;
       else if (!(bn > 0.0) || sqrt(tot[2 * k]) <= rtol * bn) f = 1;
       flags[k] = f;
     }
@@ -1198,7 +1198,8 @@ __global__ void __launch_bounds__(256) k_mgpcg_pq(const __grid_constant__ CUtens
   if (last_block<R>(v, part, cnt, red, tot) && threadIdx.x == 0) {
     for (int k = 0; k < R; ++k) {
       if (flags[k]) { S[k * 8 + 1] = 0.0; continue; }
-      if (!isfinite(tot[k]) || !(tot[k] > 0.0)) { flags[k] = 2; S[k * 8 + 1] = 0.0; continue; }
+      if (!isfinite(tot[k])) { flags[k] = 3; S[k * 8 + 1] = 0.0; continue; }
+      if (!(tot[k] > 0.0)) { flags[k] = 2; S[k * 8 + 1] = 0.0; continue; }
       S[k * 8 + 1] = S[k * 8 + 0] / tot[k];
     }
   }
@@ -1244,7 +1245,7 @@ __global__ void __launch_bounds__(256) k_mgpcg_xr(int NN, const double* __restri
       if (flags[k]) continue;
       S[k * 8 + 3] = tot[k];
       S[k * 8 + 5] += 1.0;
-      if (!isfinite(tot[k])) flags[k] = 2;
+      if (!isfinite(tot[k])) flags[k] = 3;
       else if (sqrt(tot[k]) <= S[k * 8 + 6] * S[k * 8 + 4]) flags[k] = 1;
     }
   }
@@ -1321,14 +1322,17 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
     }
-    if (mg->gexec[ri]) {
+    // never more than maxiter iterations: a remainder shorter than the
+    // captured group runs eagerly
+    const int step = std::min(kGraphIters, maxiter - it);
+    if (mg->gexec[ri] && step == kGraphIters) {
       if (cudaGraphLaunch(mg->gexec[ri], s) != cudaSuccess) { c.last_error = "multigrid PCG: graph launch"; return -2; }
       count_launch((long long)mg->gnodes[ri]);
     } else {
-      for (int q = 0; q < kGraphIters; ++q)
+      for (int q = 0; q < step; ++q)
         if (mgpcg_iter<R>(c, q & 1, s)) return -2;
     }
-    it += kGraphIters;
+    it += step;
   }
   cudaMemcpyAsync(x, mg->x, sizeof(double) * R * V, cudaMemcpyDeviceToDevice, s);
   double hs[64];
@@ -1336,7 +1340,11 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
   if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "multigrid PCG: CUDA error"; return -2; }
   for (int k = 0; k < R; ++k) {
     iters[k] = int(hs[k * 8 + 5]);
-    status[k] = hf[8] ? ST_TIMEOUT : hf[k] == 1 ? ST_OK : hf[k] == 2 ? ST_BREAKDOWN : ST_NOT_CONVERGED;
+    status[k] = hf[8] ? ST_TIMEOUT
+                : hf[k] == 1 ? ST_OK
+                : hf[k] == 2 ? ST_BREAKDOWN
+                : hf[k] == 3 ? ST_NONFINITE
+                             : ST_NOT_CONVERGED;
   }
   return 0;
 }

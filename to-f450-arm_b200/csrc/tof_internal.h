@@ -71,6 +71,7 @@ struct Ctx {
   // element matrices (FP64 dense 24x24 and the 64-block layout, FP32/FP64)
   double* Ke64 = nullptr; double* Me64 = nullptr;
   double* keb64 = nullptr; double* meb64 = nullptr;
+  double* kebabs64 = nullptr;  // |Ke| in the 64-block layout (residual rounding floor)
   float* keb32 = nullptr; float* meb32 = nullptr;
 
   uint8_t* active = nullptr;   // [NE]
@@ -90,6 +91,7 @@ struct Ctx {
   double* partials = nullptr;  // [max grid][64]
   int partial_slots = 0;
   BarrierState* bar = nullptr;
+  long long wait_ns = 0;       // wait budget of the persistent kernels (0: kWaitLimitNs)
   int* status = nullptr;       // [16] solver status words
   double* scal = nullptr;      // [256] solver scalars
   unsigned* counters = nullptr; // [16] last-block reduction counters (each kernel resets its own)
@@ -130,6 +132,7 @@ bool encode_node4_map(CUtensorMap* m, const void* base, const Grid& g, int R, bo
 // kernels (tof_kernels.cu)
 void launch_factors(Ctx& c, const double* rho, cudaStream_t s);
 void launch_diag(Ctx& c, cudaStream_t s);
+// op: 0 K, 1 M, 2 |K| (entrywise absolute values; FP64 only)
 int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, const void* b_residual,
                   cudaStream_t s);
 int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* coef, bool prev,
@@ -151,6 +154,10 @@ void launch_gram_cols(Ctx& c, bool f64, const void* A, const ColMap& ma, int na,
 void launch_quadform(const Ctx& c, int op, bool f64, const void* v, int nvec, double* out, cudaStream_t s);
 void launch_convert(const void* src, bool src64, void* dst, bool dst64, long long n, cudaStream_t s);
 void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s);
+// y += x (n floats)
+void launch_add_f32(long long n, const float* x, float* y, cudaStream_t s);
+// y = |x| (n doubles)
+void launch_abs64(long long n, const double* x, double* y, cudaStream_t s);
 void launch_add_f32_to_f64(long long n, const float* d, double* x, cudaStream_t s);
 
 // stress and fatigue (tof_stress.cu)
@@ -166,6 +173,9 @@ int launch_modal_frf(long long ndof, int m, const double* V, const double* fk_hz
                      double zeta, double* out, cudaStream_t s);
 
 // PCG (tof_pcg.cu)
+// G CTAs meet at one grid barrier that expects `expected` arrivals (more than
+// G: nobody releases it, every CTA gives up after the context's wait budget)
+int launch_barrier_selftest(Ctx& c, int G, int expected, cudaStream_t s);
 int pcg_plain64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter, int* iters, double* relres,
                 int* status, cudaStream_t s);
 int pcg_pipe32(Ctx& c, const double* b, float* d, int R, double rtol, int maxiter, int* iters, double* relres,

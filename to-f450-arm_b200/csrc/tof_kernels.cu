@@ -178,10 +178,15 @@ static int matvec_launch_t(Ctx& c, int op, const void* x, void* y, const void* b
   MatvecArgs<T> a;
   a.g = c.g;
   const bool f64 = sizeof(T) == 8;
-  a.fe = reinterpret_cast<const T*>(op == 0 ? (f64 ? (const void*)c.fK64 : (const void*)c.fK32)
+  if (op == 2 && !f64) {
+    c.last_error = "|K| products are FP64 only";
+    return -2;
+  }
+  a.fe = reinterpret_cast<const T*>(op != 1 ? (f64 ? (const void*)c.fK64 : (const void*)c.fK32)
                                             : (f64 ? (const void*)c.fM64 : (const void*)c.fM32));
-  a.keb = reinterpret_cast<const T*>(op == 0 ? (f64 ? (const void*)c.keb64 : (const void*)c.keb32)
-                                             : (f64 ? (const void*)c.meb64 : (const void*)c.meb32));
+  a.keb = reinterpret_cast<const T*>(op == 0   ? (f64 ? (const void*)c.keb64 : (const void*)c.keb32)
+                                     : op == 1 ? (f64 ? (const void*)c.meb64 : (const void*)c.meb32)
+                                               : (const void*)c.kebabs64);
   a.fix = c.fix;
   a.tip = op == 1 ? reinterpret_cast<const T*>(f64 ? (const void*)c.tip64 : (const void*)c.tip32) : nullptr;
   a.b = reinterpret_cast<const T*>(b);
@@ -700,6 +705,26 @@ __global__ void k_axpy64(long long n, const double* __restrict__ x, double* y, d
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < n) y[i] = fma(a, x[i], y[i]);
 }
+__global__ void k_add_f32(long long n, const float* __restrict__ x, float* y) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
+void launch_add_f32(long long n, const float* x, float* y, cudaStream_t s) {
+  k_add_f32<<<int((n + 255) / 256), 256, 0, s>>>(n, x, y);
+  count_launch();
+}
+
+__global__ void k_abs64(long long n, const double* __restrict__ x, double* y) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = fabs(x[i]);
+}
+
+void launch_abs64(long long n, const double* x, double* y, cudaStream_t s) {
+  k_abs64<<<int((n + 255) / 256), 256, 0, s>>>(n, x, y);
+  count_launch();
+}
+
 void launch_axpy64(long long n, const double* x, double* y, double a, cudaStream_t s) {
   k_axpy64<<<int((n + 255) / 256), 256, 0, s>>>(n, x, y, a);
   count_launch();

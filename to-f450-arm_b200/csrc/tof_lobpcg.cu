@@ -274,7 +274,8 @@ __device__ void cta_backward(double (*T)[LDA], double (*B)[LDA], const double* i
 // eigendecomposed, directions with eigenvalue below drop_tol * max are
 // discarded, and the standard problem is solved in the remaining
 // M-orthonormal basis.  One CTA, one thread per matrix element.
-// Outputs: C (n x m, row-major), theta (m), info[0] = kept rank (or -1).
+// Outputs: C (n x m, row-major), theta (m), info[0] = kept rank (or -1; -2
+// for non-finite input).
 constexpr double kCholPivot = 1e-8;
 
 __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const double* __restrict__ GK,
@@ -286,6 +287,15 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
   __shared__ int keep[kMaxBasis], order[kMaxBasis];
   __shared__ int kr;
   const int tid = threadIdx.x;
+  {
+    // non-finite Gram entries (a NaN / Inf density or start block): info -2
+    bool bad = false;
+    for (int w = tid; w < n * n; w += blockDim.x) bad = bad || !isfinite(GK[w]) || !isfinite(GM[w]);
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) info[0] = -2;
+      return;
+    }
+  }
   if (tid < n) {
     const double b = GM[tid * n + tid];
     D[tid] = b > 0.0 ? rsqrt(b) : 0.0;
@@ -522,6 +532,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   int hinfo = 0;
   cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
+  if (hinfo == -2) { c.last_error = "LOBPCG: non-finite values in the initial block's products"; return -4; }
   if (hinfo < 0) { c.last_error = "LOBPCG: initial block is rank deficient"; return -3; }
   bool conv = false;
   // K X, M X, K P, M P follow the update recurrence (S C) between refreshes.
@@ -621,11 +632,12 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     for (int j = 0; j < nmodes; ++j) fprintf(stderr, " %.2e", rres[j]);
     fprintf(stderr, " theta0 %.10e\n", hth[0]);
 #endif
+    if (hinfo == -2) { c.last_error = "LOBPCG: non-finite Rayleigh-Ritz matrices"; return -4; }
     if (hinfo < 0) { c.last_error = "LOBPCG: Rayleigh-Ritz basis rank deficient"; return -3; }
     if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
     T* W = vec<T>(B.S[cur], nb, vs);
     const int R = na <= 1 ? 1 : na <= 2 ? 2 : na <= 4 ? 4 : 8;
-    if (precond == 2) {
+    if (precond == 2 && inner_iters <= 1) {
       // W <- V-cycle(W): the FP32 multigrid approximation of K^-1
       if (mg_ensure(c, s)) return -2;
       float* r32 = mg_rhs(c, 1);
@@ -633,6 +645,26 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       launch_convert(W, f64, r32, false, (long long)na * vs, s);
       if (mg_vcycle(c, R, s, 1)) return -2;
       launch_convert(mg_out(c, 1), false, W, f64, (long long)na * vs, s);
+    } else if (precond == 2) {
+      // inner_iters multigrid cycles as a stationary iteration on K e = W:
+      // e <- e + B (W - K e), all in FP32 (the FP32 LOBPCG work area holds
+      // the kept right-hand side and the accumulated correction)
+      if (mg_ensure(c, s)) return -2;
+      float* r32 = mg_rhs(c, 1);
+      float* e32 = mg_out(c, 1);
+      float* rk = c.lw32;
+      float* ek = c.lw32 + 8 * vs;
+      if (R > na) cudaMemsetAsync(rk, 0, sizeof(float) * R * vs, s);
+      launch_convert(W, f64, rk, false, (long long)na * vs, s);
+      cudaMemcpyAsync(r32, rk, sizeof(float) * R * vs, cudaMemcpyDeviceToDevice, s);
+      if (mg_vcycle(c, R, s, 1)) return -2;
+      cudaMemcpyAsync(ek, e32, sizeof(float) * R * vs, cudaMemcpyDeviceToDevice, s);
+      for (int cyc = 1; cyc < inner_iters; ++cyc) {
+        if (launch_matvec(c, 0, false, ek, r32, R, rk, s)) return -2;
+        if (mg_vcycle(c, R, s, 1)) return -2;
+        launch_add_f32(R * vs, e32, ek, s);
+      }
+      launch_convert(ek, false, W, f64, (long long)na * vs, s);
     } else if (precond == 1) {
       // W <- (inexact) K^-1 W by block PCG (FP32)
       const size_t pblk = (size_t)c.max_rhs * vs;
@@ -688,6 +720,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
 
+  if (hinfo == -2) { c.last_error = "LOBPCG: non-finite final products"; return -4; }
   if (hinfo < 0) { c.last_error = "LOBPCG: final block rank deficient"; return -3; }
   for (int j = 0; j < nmodes; ++j) lam[j] = hth[j];
   return conv ? 0 : 1;

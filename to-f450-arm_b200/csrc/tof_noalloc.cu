@@ -3,18 +3,21 @@
 // tof_gram needs a context, whose creation allocates device memory (its
 // partial-sum buffer among it).  Some callers cannot allocate device memory
 // at the point where they need a Gram matrix: a host application whose
-// memory pool owns every byte of the GPU and forbids other allocations, code
-// running while a stream is being captured into a CUDA graph (cudaMalloc is
-// not allowed there), or a latency-critical loop that must not hit
-// cudaMalloc's implicit device synchronisation.  This entry point computes the
-// same G = A^T B with every temporary in one fixed, file-scope device array.
+// memory pool owns every byte of the GPU and forbids other allocations, or a
+// latency-critical loop that must not hit cudaMalloc's implicit device
+// synchronisation.  This entry point computes the same G = A^T B with every
+// temporary in one fixed, file-scope device array.
 //
 // Limits: na, nb <= 24 (the array holds kNaSlots partial 24 x 24 matrices)
-// and n_nodes < 2^31.  The array (about 1.1 MiB) is reserved on every GPU
-// that loads this library, for the life of the process (one copy per GPU).
-// All calls on a GPU share that copy, which keeps the last call's partial
-// sums; two calls on the same GPU whose executions overlap (for instance on
-// two streams with no ordering between them) race on it, so order them.
+// and n_nodes <= INT_MAX.  The array (about 1.1 MiB) belongs to this
+// library's device code: CUDA loads that code on a device lazily, so the
+// array takes its device memory at the first call on each device and keeps it
+// until the process exits (one copy per GPU).  That first call also looks up
+// the array's device address; make it before any stream capture and before a
+// memory pool takes over the GPU.  All calls on a GPU share that copy, which
+// keeps the last call's partial sums; two calls on the same GPU whose
+// executions overlap (for instance on two streams with no ordering between
+// them) race on it, so order them.
 #include <limits.h>
 
 #include <mutex>
@@ -49,7 +52,7 @@ __global__ void __launch_bounds__(kNaThreads) k_gram_noalloc(int NN, const T* __
   const long long vs = (long long)NN * 4;
   const int npair = na * nb;
   double acc[kNaPerThread] = {0.0, 0.0, 0.0};
-  const int nchunks = (NN + CH - 1) / CH;
+  const int nchunks = (int)(((long long)NN + CH - 1) / CH);
   const int per = (nchunks + gridDim.x - 1) / gridDim.x;
   const int c0 = blockIdx.x * per, c1 = min(nchunks, c0 + per);
   for (int ch = c0; ch < c1; ++ch) {
@@ -121,7 +124,7 @@ extern "C" int tof_gram_noalloc(long long n_nodes, int dtype, const void* A, int
     return TOF_ERR_ARG;
   }
   if (n_nodes < 1 || n_nodes > INT_MAX) {
-    set_global_error("tof_gram_noalloc: n_nodes must be in [1, 2^31 - 1]");
+    set_global_error("tof_gram_noalloc: n_nodes must be in [1, INT_MAX]");
     return TOF_ERR_ARG;
   }
   int dev = 0;
@@ -153,7 +156,7 @@ extern "C" int tof_gram_noalloc(long long n_nodes, int dtype, const void* A, int
     return TOF_ERR_CUDA;
   }
   const int CH = dtype == TOF_F64 ? 16 : 32;
-  const int nchunks = (NN + CH - 1) / CH;
+  const int nchunks = (int)(((long long)NN + CH - 1) / CH);
   const int grid = nchunks < kNaSlots ? nchunks : kNaSlots;
   if (dtype == TOF_F64)
     k_gram_noalloc<double, 16><<<grid, kNaThreads, 0, s>>>(NN, (const double*)A, na, (const double*)B, nb,

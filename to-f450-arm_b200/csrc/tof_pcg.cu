@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) k_pcg_pipe(const __grid_constant__ PipeAr
         load_factor_tile(g, tg, a.fK, sf);
         __syncthreads();
       }
-      ok = __syncthreads_and(ok && mbar_wait(mbar, phase));
+      ok = __syncthreads_and(ok && mbar_wait(mbar, phase, wait_budget(a.bar)));
       phase ^= 1;
       int tx, ty, tz, n;
       if (ok && thread_node(g, tg, tx, ty, tz, n)) {
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ Plain
         tma_load_5d(sp, &a.tmx, 0, tg.i0 - 1, tg.j0 - 1, tg.k0 - 1, 0, mbar);
       }
       if (!single) { load_factor_tile(g, tg, a.fK, sf); __syncthreads(); }
-      ok = __syncthreads_and(ok && mbar_wait(mbar, phase));
+      ok = __syncthreads_and(ok && mbar_wait(mbar, phase, wait_budget(a.bar)));
       phase ^= 1;
       int tx, ty, tz, n;
       if (ok && thread_node(g, tg, tx, ty, tz, n)) {
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(256) k_pcg_plain(const __grid_constant__ Plain
         tma_load_5d(sp, &a.tmp[pc], 0, tg.i0 - 1, tg.j0 - 1, tg.k0 - 1, 0, mbar);
       }
       if (!single) load_factor_tile(g, tg, a.fK, sf);
-      ok = __syncthreads_and(ok && mbar_wait(mbar, phase));
+      ok = __syncthreads_and(ok && mbar_wait(mbar, phase, wait_budget(a.bar)));
       phase ^= 1;
       // p_new over the whole halo box (frozen rhs: untouched)
       for (int idx = threadIdx.x; idx < R * hsr; idx += blockDim.x) {
@@ -590,7 +590,7 @@ static int pipe_launch(Ctx& c, const double* b, float* d, double rtol, int maxit
   int grid = per_sm * c.num_sms;
   if (grid > c.g.ntiles) grid = c.g.ntiles;
   if (grid > c.partial_slots) grid = c.partial_slots;
-  cudaMemsetAsync(c.bar, 0, sizeof(BarrierState), s);
+  cudaMemsetAsync(c.bar, 0, kBarrierResetBytes, s);
   void* args[] = {(void*)&a};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(c.g.TX * c.g.TY * c.g.TZ), args,
                                               smem, s);
@@ -629,10 +629,23 @@ static int plain_launch(Ctx& c, const double* b, T* x, double rtol, int maxiter,
   int grid = per_sm * c.num_sms;
   if (grid > c.g.ntiles) grid = c.g.ntiles;
   if (grid > c.partial_slots) grid = c.partial_slots;
-  cudaMemsetAsync(c.bar, 0, sizeof(BarrierState), s);
+  cudaMemsetAsync(c.bar, 0, kBarrierResetBytes, s);
   void* args[] = {(void*)&a};
   cudaError_t e = cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(c.g.TX * c.g.TY * c.g.TZ), args,
                                               smem, s);
+  count_launch();
+  if (e != cudaSuccess) { c.last_error = cudaGetErrorString(e); return -2; }
+  return 0;
+}
+
+__global__ void __launch_bounds__(32) k_barrier_selftest(BarrierState* bar, unsigned expected) {
+  grid_barrier(bar, expected);
+}
+
+int launch_barrier_selftest(Ctx& c, int G, int expected, cudaStream_t s) {
+  unsigned exp = (unsigned)expected;
+  void* args[] = {(void*)&c.bar, (void*)&exp};
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_barrier_selftest, dim3(G), dim3(32), args, 0, s);
   count_launch();
   if (e != cudaSuccess) { c.last_error = cudaGetErrorString(e); return -2; }
   return 0;

@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "ok", 1: "not converged", -1: "invalid argument", -2: "CUDA e
 
 
 class SolveStats(ctypes.Structure):
-    _fields_ = [("status", c_int), ("iters", c_int), ("outer", c_int), ("relres", c_double)]
+    _fields_ = [("status", c_int), ("iters", c_int), ("outer", c_int), ("relres", c_double), ("floor", c_double)]
 
 
 class SimpParams(ctypes.Structure):
@@ -51,6 +51,8 @@ SIGNATURES = {
                                c_int, c_int, POINTER(c_int), POINTER(P)]),
     "tof_ctx_destroy": (None, [P]),
     "tof_ctx_query": (c_longlong, [P, c_int]),
+    "tof_ctx_set_wait_limit": (c_int, [P, c_longlong]),
+    "tof_wait_selftest": (c_int, [P, c_int, P]),
     "tof_set_density": (c_int, [P, P, P]),
     "tof_set_tip_lump": (c_int, [P, POINTER(c_double), P]),
     "tof_pack": (c_int, [P, P, c_longlong, P, c_int, c_int, P]),

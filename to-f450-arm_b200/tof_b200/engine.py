@@ -61,6 +61,7 @@ class DesignContext:
         self.tile = tuple(int(self.lib.tof_ctx_query(self.h, q)) for q in (L.Q_TILE_X, L.Q_TILE_Y, L.Q_TILE_Z))
         self.active = torch.from_numpy(act.astype(bool)).to(self.device)
         self.last_stats = []
+        self.last_rc = None
 
     def close(self):
         if getattr(self, "h", None):
@@ -129,15 +130,19 @@ class DesignContext:
         x = self.zeros4(R) if x4 is None else x4.to(torch.float64).contiguous().clone()
         st = (L.SolveStats * R)()
         rc = self.lib.tof_pcg(self.h, mode, L.ptr(b4), L.ptr(x), R, float(rtol), int(maxiter), st, _stream())
-        stats = [dict(status=s.status, iters=s.iters, outer=s.outer, relres=s.relres) for s in st]
+        stats = [dict(status=s.status, iters=s.iters, outer=s.outer, relres=s.relres, floor=s.floor) for s in st]
         self.last_stats = stats
+        self.last_rc = rc
         if raise_on_error:
             L.check("tof_pcg", rc, self.h, allow=(L.TOF_OK, L.TOF_NOT_CONVERGED))
         return x, stats
 
     def lobpcg(self, X4: torch.Tensor, nmodes: int, tol=1e-5, maxiter=500, mode=L.MODE_MIXED,
-               precond=L.PRECOND_PCG, inner_iters=60, inner_rtol=1e-2, raise_on_error=True):
-        """Lowest nmodes of K x = lam M x from the start block X4 (block, NN, 4)."""
+               precond=L.PRECOND_PCG, inner_iters=60, inner_rtol=1e-2, raise_on_error=True, mg_cycles=1):
+        """Lowest nmodes of K x = lam M x from the start block X4 (block, NN, 4).
+        mg_cycles: V-cycles per preconditioner application (multigrid)."""
+        if precond == L.PRECOND_MG or mode == L.MODE_MIXED:
+            inner_iters = mg_cycles
         X = X4.to(torch.float64).contiguous().clone()
         block = X.shape[0]
         lam = (c_double * nmodes)()
@@ -147,6 +152,7 @@ class DesignContext:
                                  int(inner_iters), float(inner_rtol), ctypes.byref(st), res, _stream())
         stats = dict(status=st.status, iters=st.iters, relres=st.relres, resid=list(res))
         self.last_stats = [stats]
+        self.last_rc = rc
         if raise_on_error:
             L.check("tof_lobpcg", rc, self.h, allow=(L.TOF_OK, L.TOF_NOT_CONVERGED))
         return X[:nmodes], np.array(list(lam)), stats

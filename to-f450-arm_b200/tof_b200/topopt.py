@@ -96,6 +96,7 @@ class SIMPOptimizer:
         self.solve_rtol = fem.SOLVE_RTOL if solve_rtol is None else solve_rtol
         self.modal_tol = modal_tol
         self.modal_maxiter = modal_maxiter
+        self.modal_mg_cycles = 1              # V-cycles per LOBPCG preconditioner application
         n_lc = len(F_list) if F_list is not None else len(load_cases)
         w = np.full(n_lc, 1.0 / n_lc) if weights is None else np.asarray(weights, dtype=float)
         self.weights = w / w.sum()                                           # src/topopt.py:121-124
@@ -178,7 +179,7 @@ class SIMPOptimizer:
         self.mu_freq_cur = self.mu_freq
         self.history = {"compliance": [], "mass": [], "change": [], "vol_frac": [], "omega_1_Hz": [],
                         "mu_freq": [], "freq_violation": [], "modal_converged": [], "modal_iters": [],
-                        "pcg_iters": []}
+                        "modal_relres": [], "pcg_iters": [], "pcg_relres": []}
         self.stats = []
 
     # ------------------------------------------------------------------ #
@@ -212,12 +213,14 @@ class SIMPOptimizer:
         mid = fem._mode_id()
         maxit = self.modal_maxiter or (20000 if mid == L.MODE_FP64 else 1000)
         modes, lam, st = ctx.lobpcg(X4, n, tol=self.modal_tol, maxiter=maxit, mode=mid,
-                                    precond=L.PRECOND_MG if mid == L.MODE_MIXED else L.PRECOND_JACOBI)
+                                    precond=L.PRECOND_MG if mid == L.MODE_MIXED else L.PRECOND_JACOBI,
+                                    mg_cycles=self.modal_mg_cycles)
         # warm start: converged modes plus the previous guard vectors
         self.X4 = torch.cat([modes, X4[n:]]) if nb > n else modes.clone()
         self.stats.append(("lobpcg", st))
         self.history["modal_converged"].append(st["status"] == L.TOF_OK)
         self.history["modal_iters"].append(st["iters"])
+        self.history["modal_relres"].append(st["relres"])
         return modes, np.maximum(lam, 0.0)
 
     def _static(self, mid):
@@ -239,6 +242,7 @@ class SIMPOptimizer:
         self.u4 = u4
         self.stats.append(("pcg", st))
         self.history["pcg_iters"].append(max(s["iters"] for s in st))
+        self.history["pcg_relres"].append(max(s["relres"] for s in st))
         ce = ctx.quadform(L.OP_K, u4)
         c_dev, dc = ctx.compliance_sens(ce, self.w_dev)
         sens = self.filter.apply(dc, L.FILTER_FORWARD)       # src/topopt.py:311
@@ -337,6 +341,7 @@ class SIMPOptimizer:
                 self.history[k].append(np.nan)
         self._mark("eigen sens+penalty")
         # --- OC on design cells (src/topopt.py:377-390)
+        self.last_sensitivity = sens                         # what OC receives (full grid)
         x_d = self.x[self.design_ids]
         x_new_d = oc_update(x_d, sens[self.design_ids], self.V_e, self.target_volume, self.move)
         x_new = self.x.clone()

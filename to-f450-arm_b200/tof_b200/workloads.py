@@ -8,7 +8,10 @@ starting design), 6 tracked modes with a 500 Hz augmented-Lagrangian target,
 60 g tip mass, filter radius 1.5 voxels, vf 0.08, design start
 0.08 + U(-0.02, 0.02) (seed 0), static solves to a 1e-8 relative residual.
 The inertial load is evaluated once at the starting design and then held
-fixed, as the reference's optimiser supports design-independent loads only.
+fixed, as the reference's optimiser supports design-independent loads only;
+it is the full consistent mass applied to a unit z translation of every
+node (clamped ones included), restricted to the free DOFs by the solver,
+i.e. the rows (M @ e_z)[free] of the reference's assembled M.
 """
 from __future__ import annotations
 
@@ -33,11 +36,26 @@ def arm_simp(mode="mixed", nx=110, ny=14, nz=12, h=2e-3, vf=0.08, n_modes=6, min
                         modal_tol=modal_tol, x0_design=x0, F_list=F3 + [np.zeros(geom.n_dofs)])
     rho0 = opt.physical_density()
     rho_active = rho0[torch.as_tensor(fem.active_ids, device=rho0.device)].cpu().numpy()
-    ez = np.zeros(geom.n_dofs)
-    ez[2::3] = 1.0
-    Mr = fem.assemble_M(rho_active, C.TIP_MASS_KG, geom.motor_mount_top_nodes()) @ ez
+    Mr = consistent_mass_times_translation(fem, rho_active, C.TIP_MASS_KG, geom.motor_mount_top_nodes())
     opt.set_loads(F3 + [C.body_load_from_Mr(Mr, 3.0)])
     return geom, fem, opt
+
+
+def consistent_mass_times_translation(fem, rho_active, tip_mass_kg, tip_nodes, direction=2):
+    """M(rho) r for the unit translation r along `direction` on every DOF:
+    the SIMP / Pedersen-scaled consistent element masses (src/fem.py:362-381)
+    plus the lumped tip mass (src/fem.py:383-398), assembled on the host
+    (set-up only).  Equal to the reference's assemble_M(...) @ r."""
+    r_loc = np.zeros(24)
+    r_loc[direction::3] = 1.0
+    me_r = fem.Me_solid @ r_loc                                  # (24,)
+    m = fem._mass_simp_factor(rho_active)
+    out = np.zeros(fem.geom.n_dofs)
+    np.add.at(out, fem.elem_dof_ids, m[:, None] * me_r[None, :])
+    nodes = np.asarray(tip_nodes, dtype=np.int64)
+    if tip_mass_kg and tip_mass_kg > 0.0 and len(nodes):
+        np.add.at(out, 3 * nodes + direction, tip_mass_kg / len(nodes))
+    return out
 
 
 def arm_hollow_analysis(mode="mixed", tile=None):
