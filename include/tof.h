@@ -69,7 +69,9 @@ typedef struct {
   double floor;   /* PCG: FP64 rounding floor of relres, eps ||(|K||x| + |b|)|| / ||b||
                      (what rounding the exact solution to FP64 can leave); the
                      solve counts as converged when relres <= max(rtol, floor).
-                     LOBPCG: 0 */
+                     LOBPCG: the largest eps ||(|K| + theta M)|x||| / ||K x|| of
+                     the modes; converged when each mode's residual is at most
+                     max(tol, 10 x its floor) */
 } tof_solve_stats;
 
 /* SIMP interpolation constants: stiffness emin + (1-emin) rho^penal,

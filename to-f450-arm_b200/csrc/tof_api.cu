@@ -27,7 +27,7 @@ void launch_eig_sens(int NE, const double* rho, const double* qK, const double* 
                      SimpParams sp, double lam, double vMv_tip, double* out, double* part, double* scal,
                      cudaStream_t s);
 int lobpcg_run(Ctx& c, bool f64, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter,
-               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, int verbose,
+               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, double* floor_out,
                cudaStream_t s);
 
 // ---------------------------------------------------------------------------
@@ -639,8 +639,9 @@ int tof_lobpcg(tof_ctx* ctx, int mode, int nmodes, int block, double* X, double*
   if (block > c.max_modes) { c.last_error = "tof_lobpcg: block exceeds the context's max_modes"; return TOF_ERR_ARG; }
   int it = 0;
   double res[8] = {0};
+  double fl[8] = {0};
   const int rc = lobpcg_run(c, mode == TOF_MODE_FP64, nmodes, block, X, lam, tol, maxiter, precond,
-                            std::max(inner_iters, 1), inner_rtol, &it, res, 0, (cudaStream_t)stream);
+                            std::max(inner_iters, 1), inner_rtol, &it, res, fl, (cudaStream_t)stream);
   if (resid)
     for (int j = 0; j < nmodes; ++j) resid[j] = res[j];
   if (stats) {
@@ -650,7 +651,9 @@ int tof_lobpcg(tof_ctx* ctx, int mode, int nmodes, int block, double* X, double*
     double w = 0.0;
     for (int j = 0; j < nmodes; ++j) w = std::max(w, res[j]);
     stats->relres = w;
-    stats->floor = 0.0;
+    double f = 0.0;
+    for (int j = 0; j < nmodes; ++j) f = std::max(f, fl[j]);
+    stats->floor = f;
   }
   if (rc == -2) return TOF_ERR_CUDA;
   return rc;

@@ -44,6 +44,21 @@ constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M
 constexpr int kLobStall = 500;
 constexpr double kLobDiverge = 1e3;
 constexpr double kLobNearFloor = 1e-3;
+// Before stopping, a residual kLobRestartGrowth times above the best
+// iterate's restarts the iteration from that iterate without P (at most
+// kLobMaxRestarts times).
+constexpr double kLobRestartGrowth = 10.0;
+constexpr int kLobMaxRestarts = 3;
+// A wanted residual within this factor of its FP64 rounding floor counts as
+// converged when the floor lies above the requested tolerance.
+constexpr double kLobFloorFactor = 10.0;
+
+// y_k += theta_k m_k for nv vectors of n doubles (theta on the device)
+__global__ void k_add_scaled_cols(long long n, int nv, const double* __restrict__ theta, const double* __restrict__ m,
+                                  double* y) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n * nv) y[i] = fma(theta[i / n], m[i], y[i]);
+}
 
 // ---------------------------------------------------------------------------
 // residual W_j = KX_j - theta_j MX_j, optional Jacobi scaling, written to
@@ -486,13 +501,14 @@ static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s) {
 }
 
 int lobpcg_run(Ctx& c, bool f64, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter,
-               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, int verbose,
+               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, double* floor_out,
                cudaStream_t s);
 
 // Implementation templated on the vector type.
 template <typename T>
 static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter, int precond,
-                       int inner_iters, double inner_rtol, int* iters_out, double* resid_out, cudaStream_t s) {
+                       int inner_iters, double inner_rtol, int* iters_out, double* resid_out, double* floor_out,
+                       cudaStream_t s) {
   const bool f64 = sizeof(T) == 8;
   const long long vs = (long long)c.g.NN * 4;
   const int NN = c.g.NN;
@@ -588,6 +604,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     return 0;
   };
   double best = INFINITY;
+  int restarts = 0, ncols_prev = 0;
   double best_res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int it_best = 0;
   bool use_best = false;
@@ -617,11 +634,25 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       na = active_map();
       if (residual()) return -2;
     }
+    // the previous Rayleigh-Ritz step dropped directions (SVQB): the basis
+    // had become ill-conditioned, so the next one leaves P out (restart)
+    bool drop_p = hinfo > 0 && hinfo < ncols_prev;
     if (worst < best) {
       best = worst;
       it_best = it;
       for (int j = 0; j < nmodes; ++j) best_res[j] = rres[j];
       cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+    } else if (best < kLobNearFloor && worst > kLobRestartGrowth * best && restarts < kLobMaxRestarts) {
+      // the residual grew well past the best iterate: continue from the best
+      // iterate with fresh products and without P
+      ++restarts;
+      cudaMemcpyAsync(B.S[cur], X6, sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+      if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
+      if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
+      for (int j = 0; j < nmodes; ++j) locked[j] = false;
+      na = active_map();
+      if (residual()) return -2;
+      drop_p = true;
     } else if (best < kLobNearFloor &&
                (worst > kLobDiverge * best || it - it_best >= std::max(kLobStall, it_best))) {
       use_best = true;
@@ -683,9 +714,10 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     int ncols = 0;
     for (int j = 0; j < nb; ++j) cols.col[ncols++] = j;
     for (int k = 0; k < na; ++k) cols.col[ncols++] = nb + k;
-    if (it > 0)
+    if (it > 0 && !drop_p)
       for (int k = 0; k < na; ++k) cols.col[ncols++] = 2 * nb + act[k];
     for (int k = ncols; k < 24; ++k) cols.col[k] = 0;
+    ncols_prev = ncols;
     launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s, c.gram_part_m);
     lob_small_eig(c, ncols, nb, drop, s);
     cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -715,7 +747,23 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     launch_lob_update<double>(NN, nb, nb, ident, vs, X6, KX6, MX6, C, scratch, scratch + 3LL * c.max_modes * vs,
                               scratch + 6LL * c.max_modes * vs, s);
     cudaMemcpyAsync(out, scratch, sizeof(double) * nmodes * vs, cudaMemcpyDeviceToDevice, s);
+    // rounding floor of each returned residual: eps ||(|K| + theta M)|x|||
+    // / ||K x|| (M has no negative entries); the current-iterate buffers are
+    // free by now
+    double* ax = (double*)B.S[cur];
+    double* y = (double*)B.KS[cur];
+    double* mx = (double*)B.MS[cur];
+    launch_abs64((long long)nmodes * vs, out, ax, s);
+    if (launch_matvec(c, 2, true, ax, y, nmodes, nullptr, s)) return -2;
+    if (launch_matvec(c, 1, true, ax, mx, nmodes, nullptr, s)) return -2;
+    k_add_scaled_cols<<<int((4LL * NN * nmodes + 255) / 256), 256, 0, s>>>(4LL * NN, nmodes, th, mx, y);
+    count_launch();
+    launch_gram(c, true, y, nmodes, y, nmodes, c.gram + 6 * 576, s, c.gram_part_m);
+    launch_gram(c, true, scratch + 3LL * c.max_modes * vs, nmodes, scratch + 3LL * c.max_modes * vs, nmodes,
+                c.gram + 6 * 576 + 64, s, c.gram_part_m);
   }
+  double gfl[2][64];
+  cudaMemcpyAsync(gfl, c.gram + 6 * 576, sizeof(gfl), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(hth, th, sizeof(double) * nb, cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
@@ -723,7 +771,18 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (hinfo == -2) { c.last_error = "LOBPCG: non-finite final products"; return -4; }
   if (hinfo < 0) { c.last_error = "LOBPCG: final block rank deficient"; return -3; }
   for (int j = 0; j < nmodes; ++j) lam[j] = hth[j];
-  return conv ? 0 : 1;
+  // converged: every wanted residual at tol, or at a small multiple of its
+  // FP64 rounding floor where that lies above tol (the lowest modes of soft
+  // SIMP designs, eps lambda_max / lambda_1 ~ 1e-6)
+  bool at_floor = true;
+  for (int j = 0; j < nmodes; ++j) {
+    const double kx = sqrt(gfl[1][j * nmodes + j]);
+    const double fl = kx > 0.0 ? 2.220446049250313e-16 * sqrt(gfl[0][j * nmodes + j]) / kx : 0.0;
+    if (floor_out) floor_out[j] = fl;
+    const double r = use_best ? best_res[j] : rres[j];
+    if (!(r <= std::max(tol, kLobFloorFactor * fl))) at_floor = false;
+  }
+  return (conv || at_floor) ? 0 : 1;
 }
 
 // The block vectors are FP64 in both modes: FP32 block vectors (with FP64
@@ -731,11 +790,11 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
 // cantilever (the K X / M X recurrences drift by eps_32 * cond), so the mixed
 // mode puts FP32 where it is safe, in the multigrid preconditioner.
 int lobpcg_run(Ctx& c, bool f64, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter,
-               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, int,
+               int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, double* floor_out,
                cudaStream_t s) {
   if (!f64) precond = 2;
   return lobpcg_impl<double>(c, nmodes, nb, X64, lam, tol, maxiter, precond, inner_iters, inner_rtol, iters_out,
-                             resid_out, s);
+                             resid_out, floor_out, s);
 }
 
 }  // namespace tof

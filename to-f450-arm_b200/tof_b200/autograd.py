@@ -76,8 +76,14 @@ class SIMPObjective:
         precond = L.PRECOND_MG if self.mode_id == L.MODE_MIXED else L.PRECOND_JACOBI
         modes, lam, st = ctx.lobpcg(self.X4, n, tol=self.modal_tol, maxiter=self.modal_maxiter,
                                     mode=self.mode_id, precond=precond)
-        if st["status"] != L.TOF_OK:
-            raise L.SolverError("tof_lobpcg", st["status"], "modal solve did not reach modal_tol")
+        # LOBPCG stops at the best iterate when its residual stalls (on the
+        # softest SIMP designs the lowest modes stall near 1e-5); eigenvalues
+        # are second-order in that residual, so a stall within 100x of the
+        # tolerance is accepted, anything worse is an error
+        if st["status"] < 0 or st["relres"] > 100.0 * self.modal_tol:
+            raise L.SolverError("tof_lobpcg", st["status"],
+                                f"modal solve stopped at residual {st['relres']:.2e} (tolerance {self.modal_tol:.1e})")
+        self.modal_stats = st
         self.X4 = torch.cat([modes, self.X4[n:]]) if nb > n else modes.clone()
         return modes, np.maximum(lam, 0.0)
 

@@ -150,7 +150,7 @@ class DesignContext:
         st = L.SolveStats()
         rc = self.lib.tof_lobpcg(self.h, mode, nmodes, block, L.ptr(X), lam, float(tol), int(maxiter), precond,
                                  int(inner_iters), float(inner_rtol), ctypes.byref(st), res, _stream())
-        stats = dict(status=st.status, iters=st.iters, relres=st.relres, resid=list(res))
+        stats = dict(status=st.status, iters=st.iters, relres=st.relres, floor=st.floor, resid=list(res))
         self.last_stats = [stats]
         self.last_rc = rc
         if raise_on_error:
