@@ -119,6 +119,9 @@ static cudaError_t dalloc(Ctx& c, T** p, size_t n) {
 
 static void free_ctx(Ctx& c) {
   mg_destroy(c);
+  for (cudaEvent_t& e : c.lob_ev)
+    if (e) { cudaEventDestroy(e); e = nullptr; }
+  if (c.lob_pin) { cudaFreeHost(c.lob_pin); c.lob_pin = nullptr; }
   void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.kebabs64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
                   c.fK64, c.fM64, c.fK32, c.fM32, c.rho, c.dK64, c.dM64, c.dinvK64, c.dinvK32, c.partials,
                   c.bar, c.status, c.scal, c.counters, c.pw32, c.pw64, c.lw32, c.lw64, c.gram, c.gram_part,
@@ -264,6 +267,8 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.gram_part_m, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.counters_m, 16)); A(dalloc(c, &c.status_m, 16)); A(dalloc(c, &c.scal_m, 256));
+  A(cudaHostAlloc(&c.lob_pin, 3 * 256, cudaHostAllocDefault));
+  for (cudaEvent_t& ev : c.lob_ev) A(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
   if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error.str());
   mg_capture_all(c);

@@ -583,19 +583,35 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   };
   double worst = 0.0;
   bool finite = true;
-  auto residual = [&]() -> int {
+  // The host reads each iteration's residual norms one iteration late: the
+  // residual kernel of iteration k copies its norms (and the rank word of
+  // the Rayleigh-Ritz step before it) into a pinned slot and records an
+  // event; the host launches the rest of iteration k, then waits for that
+  // event only when it prepares iteration k + 1, so the GPU always has
+  // queued work and the host never drains the stream.  Locking, restart and
+  // stopping decisions therefore act one iteration later than they were
+  // observed.  Slots 0 / 1 alternate; slot 2 is for synchronous reads.
+  struct LobSlot { double r[16]; double th[8]; int info; int pad; };
+  LobSlot* hp = reinterpret_cast<LobSlot*>(c.lob_pin);
+  auto launch_resid = [&](int slot) {
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
     k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, (T*)B.S[cur],
                                            wslot, c.gram_part_m, c.counters_m, rn);
     count_launch();
-    cudaMemcpyAsync(hr, rn, sizeof(hr), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(hth, th, sizeof(hth), cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
+    cudaMemcpyAsync(hp[slot].r, rn, sizeof(hp[slot].r), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hp[slot].th, th, sizeof(hp[slot].th), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hp[slot].info, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaEventRecord(c.lob_ev[slot], s);
+  };
+  auto read_resid = [&](int slot) -> int {
+    if (cudaEventSynchronize(c.lob_ev[slot]) != cudaSuccess) { c.last_error = "LOBPCG: CUDA error"; return -2; }
     worst = 0.0;
     finite = true;
+    hinfo = hp[slot].info;
+    for (int j = 0; j < 8; ++j) hth[j] = hp[slot].th[j];
     for (int j = 0; j < nmodes; ++j) {
-      const double r = sqrt(hr[2 * j]) / fmax(sqrt(hr[2 * j + 1]), 1e-300);
+      const double r = sqrt(hp[slot].r[2 * j]) / fmax(sqrt(hp[slot].r[2 * j + 1]), 1e-300);
       if (!isfinite(r)) finite = false;
       worst = fmax(worst, r);
       rres[j] = r;
@@ -603,45 +619,33 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     }
     return 0;
   };
+  auto residual = [&]() -> int {       // synchronous: launch and read at once
+    launch_resid(2);
+    return read_resid(2);
+  };
   double best = INFINITY;
   int restarts = 0, ncols_prev = 0;
   double best_res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int it_best = 0;
   bool use_best = false;
   double* X6 = c.lw64;                         // holds the best iterate (free until the final step)
-  for (it = 0; it < maxiter; ++it) {
-    const bool fresh = it > 0 && it % kLobRefresh == 0;
-    if (fresh && refresh()) return -2;
-    int na = active_map();
-    if (residual()) return -2;
+  int pending = -1;                            // slot of a residual launched but not yet read
+  // Bookkeeping on the residual of the iterate before the current one (in
+  // S[cur ^ 1] until this iteration's update).  Returns 1 to stop the
+  // iteration, < 0 on error; sets drop_p for a restart.
+  bool drop_p = false;
+  auto observe = [&](int itk) -> int {
     if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
-    bool changed = false, all = true;
-    for (int j = 0; j < nmodes; ++j) {
-      if (!locked[j] && rres[j] <= tol) { locked[j] = true; changed = true; }
-      all = all && locked[j];
-    }
-    if (all) {                                 // confirm on fresh products
-      if (!fresh && it > 0 && refresh()) return -2;
-      active_map();
-      if (residual()) return -2;
-      bool reopened = false;
-      for (int j = 0; j < nmodes; ++j)
-        if (!(rres[j] <= tol)) { locked[j] = false; reopened = true; }
-      if (!reopened) { conv = true; break; }
-      changed = true;
-    }
-    if (changed) {                             // W of the new active set
-      na = active_map();
-      if (residual()) return -2;
-    }
-    // the previous Rayleigh-Ritz step dropped directions (SVQB): the basis
-    // had become ill-conditioned, so the next one leaves P out (restart)
-    bool drop_p = hinfo > 0 && hinfo < ncols_prev;
+    if (hinfo == -2) { c.last_error = "LOBPCG: non-finite Rayleigh-Ritz matrices"; return -4; }
+    if (hinfo < 0) { c.last_error = "LOBPCG: Rayleigh-Ritz basis rank deficient"; return -3; }
+    // the Rayleigh-Ritz step before that iterate dropped directions (SVQB):
+    // the basis had become ill-conditioned, so the next one leaves P out
+    if (hinfo > 0 && hinfo < ncols_prev) drop_p = true;
     if (worst < best) {
       best = worst;
-      it_best = it;
+      it_best = itk;
       for (int j = 0; j < nmodes; ++j) best_res[j] = rres[j];
-      cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+      cudaMemcpyAsync(X6, B.S[cur ^ 1], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
     } else if (best < kLobNearFloor && worst > kLobRestartGrowth * best && restarts < kLobMaxRestarts) {
       // the residual grew well past the best iterate: continue from the best
       // iterate with fresh products and without P
@@ -650,22 +654,53 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
       if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
       for (int j = 0; j < nmodes; ++j) locked[j] = false;
-      na = active_map();
-      if (residual()) return -2;
       drop_p = true;
     } else if (best < kLobNearFloor &&
-               (worst > kLobDiverge * best || it - it_best >= std::max(kLobStall, it_best))) {
+               (worst > kLobDiverge * best || itk - it_best >= std::max(kLobStall, it_best))) {
       use_best = true;
-      break;
+      return 1;
     }
+    return 0;
+  };
+  int ncols_at[2] = {nb, nb};                  // basis size of each iteration's Rayleigh-Ritz step
+  for (it = 0; it < maxiter; ++it) {
+    const bool fresh = it > 0 && it % kLobRefresh == 0;
+    if (fresh && refresh()) return -2;
+    if (pending >= 0) {
+      if (read_resid(pending)) return -2;      // iteration it - 1 (rank word of the step before it)
+      pending = -1;
+      ncols_prev = it >= 2 ? ncols_at[(it - 2) & 1] : nb;
+      bool all = true;
+      for (int j = 0; j < nmodes; ++j) {
+        if (!locked[j] && rres[j] <= tol) locked[j] = true;
+        all = all && locked[j];
+      }
+      bool confirmed_open = false;
+      if (all && finite) {                     // confirm on fresh products of the current iterate
+        if (!fresh && refresh()) return -2;
+        active_map();
+        if (residual()) return -2;
+        bool reopened = false;
+        for (int j = 0; j < nmodes; ++j)
+          if (!(rres[j] <= tol)) { locked[j] = false; reopened = true; }
+        if (!reopened) { conv = true; break; }
+        if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
+        confirmed_open = true;
+      }
+      if (!confirmed_open) {
+        const int o = observe(it - 1);
+        if (o < 0) return o;
+        if (o > 0) break;
+      }
+    }
+    int na = active_map();
+    launch_resid(it & 1);
+    pending = it & 1;
 #ifdef TOF_LOB_TRACE
-    fprintf(stderr, "lobpcg it %d rank %d active %d fresh %d worst %.3e res", it, hinfo, na, int(fresh), worst);
+    fprintf(stderr, "lobpcg it %d rank %d active %d fresh %d worst(prev) %.3e res", it, hinfo, na, int(fresh), worst);
     for (int j = 0; j < nmodes; ++j) fprintf(stderr, " %.2e", rres[j]);
     fprintf(stderr, " theta0 %.10e\n", hth[0]);
 #endif
-    if (hinfo == -2) { c.last_error = "LOBPCG: non-finite Rayleigh-Ritz matrices"; return -4; }
-    if (hinfo < 0) { c.last_error = "LOBPCG: Rayleigh-Ritz basis rank deficient"; return -3; }
-    if (!finite) { c.last_error = "LOBPCG: non-finite residual"; return -4; }
     T* W = vec<T>(B.S[cur], nb, vs);
     const int R = na <= 1 ? 1 : na <= 2 ? 2 : na <= 4 ? 4 : 8;
     if (precond == 2 && inner_iters <= 1) {
@@ -717,13 +752,19 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (it > 0 && !drop_p)
       for (int k = 0; k < na; ++k) cols.col[ncols++] = 2 * nb + act[k];
     for (int k = ncols; k < 24; ++k) cols.col[k] = 0;
-    ncols_prev = ncols;
+    drop_p = false;
+    ncols_at[it & 1] = ncols;
     launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s, c.gram_part_m);
     lob_small_eig(c, ncols, nb, drop, s);
-    cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, s);
     launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
                          (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
     cur ^= 1;
+  }
+  if (pending >= 0 && !conv && !use_best) {    // the last iterate's residual, not yet read
+    if (read_resid(pending)) return -2;
+    ncols_prev = it >= 2 ? ncols_at[(it - 2) & 1] : nb;
+    const int o = observe(it - 1);
+    if (o < 0) return o;
   }
   if (iters_out) *iters_out = it;
   if (!conv && it >= maxiter && worst > best) use_best = true;
