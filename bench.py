@@ -182,34 +182,56 @@ def time_steps(fn, n, flush_buf, torch):
     return total, per
 
 
-def measure_kernel(ctx, torch, L, R=4, reps=50):
-    """Average device time of the fine-level FP32 matvec (the multigrid
-    smoother kernel) over `reps` back-to-back launches replayed from a CUDA
-    graph, so host overhead does not enter."""
-    x = ctx.pack(torch.randn(R, ctx.N, dtype=torch.float64, device=ctx.device), dtype=torch.float32)
-    y = torch.empty_like(x)
+def _peak_hbm():
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        return float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def kernel_rooflines(ctx, torch, L, reps=100):
+    """Live per-launch device time (tof_time_kernel: a CUDA graph of `reps`
+    back-to-back launches between CUDA events on the current stream) and the
+    HBM roofline fraction of the kernels that dominate a design iteration,
+    largest share first: the coarse-level multigrid operator (levels 1 and
+    2; 4 vectors as in the static block solve, 8 as in the LOBPCG
+    preconditioner), the Rayleigh-Ritz eigensolver, the fine-level FP32
+    matrix-free operator (8 and 4 vectors).
+    `traffic`: DRAM bytes per launch from the committed ncu capture
+    (profiles/roofline_traffic.json), where captured."""
+    import ctypes
     lib = ctx.lib
-    s = torch.cuda.current_stream()
-    for _ in range(3):
-        lib.tof_matvec(ctx.h, L.OP_K, L.F32, L.ptr(x), L.ptr(y), R, L.c_void_p(s.cuda_stream))
-    torch.cuda.synchronize()
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(g):
-        cs = L.c_void_p(torch.cuda.current_stream().cuda_stream)
-        for _ in range(reps):
-            lib.tof_matvec(ctx.h, L.OP_K, L.F32, L.ptr(x), L.ptr(y), R, cs)
-    g.replay()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(4):
-        g.replay()
-    e1.record()
-    e1.synchronize()
-    per_launch = e0.elapsed_time(e1) / 1e3 / (4 * reps)
-    del g
-    return per_launch
+    peak, src = _peak_hbm()
+    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    traffic = json.load(open(tpath)) if os.path.exists(tpath) else {}
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n_levels = ctx.lib.tof_mg_query(ctx.h, -1, None, None, s)
+    cases = [("k_mgs_op level 1, 4 vectors", "k_mgs_op_l1_r4", L.KERNEL_MG_LEVEL_OP, 1, 4, "latency (L2-resident level)"),
+             ("k_mgs_op level 1, 8 vectors", "k_mgs_op_l1_r8", L.KERNEL_MG_LEVEL_OP, 1, 8, "latency (L2-resident level)"),
+             ("k_mgs_op level 2, 4 vectors", "k_mgs_op_l2_r4", L.KERNEL_MG_LEVEL_OP, 2, 4, "latency (L2-resident level)"),
+             ("k_small_eig (Rayleigh-Ritz, one CTA)", "k_small_eig", L.KERNEL_RAYLEIGH_RITZ, 0, 1,
+              "latency (one CTA, barrier-separated Jacobi rounds)"),
+             ("k_matvec<float,8> fine level", "k_matvec_f32_r8", L.KERNEL_MATVEC_F32, 0, 8, "FP32 issue / L2"),
+             ("k_matvec<float,4> fine level", "k_matvec_f32_r4", L.KERNEL_MATVEC_F32, 0, 4, "FP32 issue / L2")]
+    out = []
+    for name, key, kind, level, R, why in cases:
+        if kind == L.KERNEL_MG_LEVEL_OP and level > n_levels - 2:
+            continue
+        t = L.KernelTiming()
+        rc = lib.tof_time_kernel(ctx.h, kind, level, R, reps, ctypes.byref(t), s)
+        if rc != 0:
+            continue
+        us = t.us
+        ach = t.bytes / (us * 1e-6) / 1e9 if us > 0 else 0.0
+        out.append({"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "traffic": traffic.get(key), "peak_source": src, "launch_us": us,
+                    "algorithmic_bytes_per_launch": t.bytes, "flops_per_launch": t.flops,
+                    "achieved_tflops": t.flops / (us * 1e-6) / 1e12 if us > 0 else 0.0, "units": int(t.units),
+                    "what_bounds_it": why})
+    t = L.KernelTiming()
+    if lib.tof_time_kernel(ctx.h, L.KERNEL_VCYCLE, 0, 8, 20, ctypes.byref(t), s) == 0 and out:
+        out[0]["vcycle_r8_us"] = t.us
+    return out
 
 
 def solver_comparison(torch, L, C):
@@ -394,26 +416,12 @@ def own_arm(a, rank, world, local_rank):
            "h2d_bytes_per_step": int(n_design * 8 + F_host.numel() * 8),
            "d2h_bytes_per_step": int(n_design * 8 + 8 * 4)}
 
-    # ---- dominant kernel roofline (fine-level FP32 matvec, 4 vectors)
-    ctx = opt.ctx
-    t_k = measure_kernel(ctx, torch, L, R=4)
-    Ne, NN, Rv = ctx.NE, ctx.NN, 4
-    alg_bytes = 4 * (2 * 3 * NN * Rv) + 4 * Ne            # u read + y written (3 comps), one factor per element
-    alg_flops = 1152 * Ne * Rv
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    peak, peak_src = 6650.0, "fallback"
-    if os.path.exists(peaks_path):
-        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    achieved = alg_bytes / t_k / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_src,
-                "kernel": "k_matvec<float,4>: fine-level matrix-free K x (multigrid smoother / residual)",
-                "launch_us": t_k * 1e6, "algorithmic_bytes_per_launch": alg_bytes,
-                "flops_per_launch": alg_flops, "achieved_fp32_tflops": alg_flops / t_k / 1e12}
+    # ---- roofline of the kernels with the largest shares of a design
+    # iteration's device time (profiles/simp_iteration_arm_launches.md):
+    # each timed live, with CUDA events around a graph of back-to-back
+    # launches on this stream, on the state the timed steps left behind
+    roofline_top = kernel_rooflines(opt.ctx, torch, L)
+    roofline = dict(roofline_top[0]) if roofline_top else None
 
     line = {"metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": total / a.steps * 1e3, "higher_is_better": True,
@@ -422,7 +430,7 @@ def own_arm(a, rank, world, local_rank):
                        "load_cases": len(opt.F_list), "modes": opt.n_modes_track, "pcg_rtol": 1e-8,
                        "l2": "flushed between timed steps (256 MiB write outside the timed events)",
                        "parallelism": "replicas" if world > 1 else "single"},
-            "e2e": e2e, "roofline": roofline, "gpu_launches": int(launches),
+            "e2e": e2e, "roofline": roofline, "roofline_top": roofline_top, "gpu_launches": int(launches),
             "step_ms": [p * 1e3 for p in per],
             "history": {"compliance": hist["compliance"][-a.steps:], "omega_1_Hz": hist["omega_1_Hz"][-a.steps:]},
             "convergence": {"design_iterations": [a.warmup + 1, a.warmup + a.steps],

@@ -163,6 +163,30 @@ int tof_diag(tof_ctx* ctx, int op, double* out, void* stream);
 int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double rtol, int maxiter,
             tof_solve_stats* stats, void* stream);
 
+/* Kernel timing (diagnostics; no reference counterpart): `reps` launches of
+ * one kernel, recorded into a CUDA graph on `stream` (not the legacy default
+ * stream), replayed once to warm up and once between CUDA events; out->us is
+ * the average device time of one launch, out->bytes / out->flops the
+ * algorithmic traffic and arithmetic of one launch (0 where not meaningful),
+ * out->units the nodes / elements / basis size it covers.  Kernels:
+ * TOF_KERNEL_MATVEC_F32 (matrix-free FP32 K x on the fine grid, nvec
+ * vectors, the multigrid smoother's operator), TOF_KERNEL_MG_LEVEL_OP (the
+ * assembled-stencil operator of multigrid level `level` >= 1 in its
+ * smoothing form), TOF_KERNEL_RAYLEIGH_RITZ (the LOBPCG Rayleigh-Ritz
+ * eigensolver on the Gram matrices of the context's last LOBPCG iteration),
+ * TOF_KERNEL_VCYCLE (a whole V-cycle, all its kernels).  The multigrid
+ * kernels need the hierarchy of the current density (tof_mg_setup).  Work
+ * vectors of the context are overwritten; the graph is created and
+ * destroyed inside the call. */
+enum { TOF_KERNEL_MATVEC_F32 = 0, TOF_KERNEL_MG_LEVEL_OP = 1, TOF_KERNEL_RAYLEIGH_RITZ = 2, TOF_KERNEL_VCYCLE = 3 };
+typedef struct {
+  double us;
+  double bytes;
+  double flops;
+  long long units;
+} tof_kernel_timing;
+int tof_time_kernel(tof_ctx* ctx, int kernel, int level, int nvec, int reps, tof_kernel_timing* out, void* stream);
+
 /* Multigrid preconditioner introspection (no reference counterpart: the
  * reference preconditions with diag(K) only).  tof_mg_query: number of
  * levels (return value); for `level` >= 0 also its element dims (dims[3]) and

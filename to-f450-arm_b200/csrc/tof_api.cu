@@ -130,6 +130,24 @@ static void free_ctx(Ctx& c) {
     if (p) cudaFree(p);
 }
 
+// CUDA loads device functions lazily, at their first launch; a first launch
+// in the middle of a solve (a block size reached only once soft locking has
+// removed columns, say) then stalls that solve for tens of milliseconds.
+// The first context created on each device loads every kernel up front.
+static void preload_all_kernels(int dev) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  std::lock_guard<std::mutex> g(mu);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  preload_kernels_core();
+  preload_kernels_gmg();
+  preload_kernels_lobpcg();
+  preload_kernels_pcg();
+  preload_kernels_topopt();
+  cudaGetLastError();
+  done[dev] = true;
+}
+
 extern "C" {
 
 int tof_version(void) { return 100; }
@@ -192,6 +210,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
     return TOF_ERR_CUDA;
   };
   if (cudaGetDevice(&c.dev) != cudaSuccess) return fail("no CUDA device");
+  preload_all_kernels(c.dev);
   cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.dev);
 
   // ---- host-side bookkeeping: active set, fixed + ghost DOFs, tip lump
@@ -263,7 +282,7 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.pw64, 8 * R * V));
   A(dalloc(c, &c.lw32, 18 * MM * V));
   A(dalloc(c, &c.lw64, 21 * MM * V));
-  A(dalloc(c, &c.gram, 8 * 576));
+  A(dalloc(c, &c.gram, 12 * 576));
   A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.gram_part_m, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.counters_m, 16)); A(dalloc(c, &c.status_m, 16)); A(dalloc(c, &c.scal_m, 256));
@@ -605,6 +624,95 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
     }
   }
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// kernel timing (diagnostics)
+// ---------------------------------------------------------------------------
+int tof_time_kernel(tof_ctx* ctx, int kernel, int level, int nvec, int reps, tof_kernel_timing* out, void* stream) {
+  if (!ctx || !out || reps < 1 || reps > 1000 || !stream) return TOF_ERR_ARG;
+  Ctx& c = ctx->c;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int R = nvec;
+  if (R != 1 && R != 2 && R != 4 && R != 8) { c.last_error = "tof_time_kernel: nvec must be 1, 2, 4 or 8"; return TOF_ERR_ARG; }
+  const size_t V = (size_t)c.g.NN * 4;
+  const size_t blk = (size_t)c.max_rhs * V;
+  double bytes = 0.0, flops = 0.0;
+  long long units = 0;
+  int n_rr = 0;
+  auto launch_once = [&]() -> int {
+    switch (kernel) {
+      case TOF_KERNEL_MATVEC_F32:
+        if (R > c.max_rhs) return -1;
+        units = c.g.NE;
+        return launch_matvec(c, 0, false, c.pw32, c.pw32 + blk, R, nullptr, s);
+      case TOF_KERNEL_MG_LEVEL_OP:
+        return mg_launch_level_op(c, level, R, s, &units);
+      case TOF_KERNEL_RAYLEIGH_RITZ:
+        return lob_launch_rayleigh_ritz(c, s, &n_rr);
+      case TOF_KERNEL_VCYCLE:
+        units = c.g.NN;
+        return mg_vcycle(c, R, s, 0);
+    }
+    c.last_error = "tof_time_kernel: unknown kernel";
+    return -1;
+  };
+  if ((kernel == TOF_KERNEL_MG_LEVEL_OP || kernel == TOF_KERNEL_VCYCLE) && mg_ensure(c, s)) {
+    c.last_error = "tof_time_kernel: multigrid setup failed";
+    return TOF_ERR_CUDA;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  capturing() = true;
+  int rc = 0;
+  for (int r = 0; r < reps && rc == 0; ++r) rc = launch_once();
+  capturing() = false;
+  const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+  if (rc != 0 || ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (ec != cudaSuccess && rc == 0) c.last_error = std::string("tof_time_kernel: capture: ") + cudaGetErrorString(ec);
+    return rc == -1 ? TOF_ERR_ARG : TOF_ERR_CUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&ge, graph, 0);
+  cudaGraphDestroy(graph);
+  CUDA_TRY(ei);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  float ms = 0.f;
+  cudaError_t e = cudaGraphLaunch(ge, s);                       // warm
+  if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+  if (e == cudaSuccess) e = cudaGraphLaunch(ge, s);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(ge);
+  CUDA_TRY(e);
+  switch (kernel) {
+    case TOF_KERNEL_MATVEC_F32:     // x read, y written (3 components), one factor per element
+      bytes = 4.0 * (2.0 * 3.0 * c.g.NN * R) + 4.0 * c.g.NE;
+      flops = 1152.0 * c.g.NE * R;
+      break;
+    case TOF_KERNEL_MG_LEVEL_OP:    // 27 3x3 FP32 stencil blocks per node; x, b, y_prev read, y written
+      bytes = double(units) * (972.0 + 64.0 * R);
+      flops = double(units) * 486.0 * R;
+      break;
+    case TOF_KERNEL_RAYLEIGH_RITZ:  // two n x n FP64 Gram matrices in, C and theta out
+      units = n_rr;
+      bytes = 8.0 * (2.0 * n_rr * n_rr + n_rr * c.lob_last_m + c.lob_last_m);
+      break;
+    default:
+      break;
+  }
+  out->us = 1e3 * double(ms) / reps;
+  out->bytes = bytes;
+  out->flops = flops;
+  out->units = units;
+  return TOF_OK;
 }
 
 int tof_mg_query(tof_ctx* ctx, int level, int* dims, float* omega, void* stream) {

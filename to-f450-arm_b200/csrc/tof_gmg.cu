@@ -1051,6 +1051,21 @@ int mg_apply(Ctx& c, const float* r, float* e, int R, cudaStream_t s) {
   return cudaMemcpyAsync(e, mg->buf[0][0].e, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? 0 : -2;
 }
 
+int mg_launch_level_op(Ctx& c, int level, int R, cudaStream_t s, long long* nodes) {
+  MG* mg = c.mg;
+  if (!mg || mg->dirty) { c.last_error = "the multigrid hierarchy is not set up (tof_mg_setup)"; return -1; }
+  if (level < 1 || level > mg->nlev - 2) { c.last_error = "level must be a stencil level (1 .. levels - 2)"; return -1; }
+  if ((R != 1 && R != 2 && R != 4 && R != 8) || R > mg->maxR) {
+    c.last_error = "R must be 1, 2, 4 or 8 and at most the context's max_rhs";
+    return -1;
+  }
+  MGLevel& L = mg->L[level];
+  MGBuf& B = mg->buf[0][level];
+  *nodes = L.NN;
+  launch_mgs_op(view(L), R, B.e, B.r, B.e2, mg->coef + level * kCoefStride + 3, 3, s);
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
 void mg_mark_dirty(Ctx& c) {
   if (c.mg) c.mg->dirty = true;
 }
@@ -1359,6 +1374,22 @@ int pcg_mg64(Ctx& c, const double* b, double* x, int R, double rtol, int maxiter
   }
   c.last_error = "multigrid PCG: nrhs must be 1, 2, 4 or 8";
   return -1;
+}
+
+// Load every kernel of this file now (CUDA loads device functions lazily,
+// at first use, and a first use in the middle of a solve stalls it).
+void preload_kernels_gmg() {
+  auto touch = [](auto f) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(f));
+  };
+  touch(k_mg_galerkin); touch(k_mg_diag); touch(k_mg_stencil); touch(k_mg_coarse_setup);
+  touch(k_mg_coarse_inverse); touch(k_mgs_op); touch(k_mg_jacobi0); touch(k_mg_power_init); touch(k_mg_scale_dinv);
+  touch(k_mg_lambda); touch(k_mg_restrict); touch(k_mg_prolong); touch(k_mg_coarse_solve);
+  touch(k_mgpcg_init<1>); touch(k_mgpcg_init<2>); touch(k_mgpcg_init<4>); touch(k_mgpcg_init<8>);
+  touch(k_mgpcg_zrz<1>); touch(k_mgpcg_zrz<2>); touch(k_mgpcg_zrz<4>); touch(k_mgpcg_zrz<8>);
+  touch(k_mgpcg_pq<1>); touch(k_mgpcg_pq<2>); touch(k_mgpcg_pq<4>); touch(k_mgpcg_pq<8>);
+  touch(k_mgpcg_xr<1>); touch(k_mgpcg_xr<2>); touch(k_mgpcg_xr<4>); touch(k_mgpcg_xr<8>);
 }
 
 }  // namespace tof

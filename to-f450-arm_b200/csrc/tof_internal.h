@@ -24,6 +24,13 @@ bool& capturing();   // per host thread
 inline void count_launch(long long n = 1) {
   if (!capturing()) launch_counter().fetch_add(n, std::memory_order_relaxed);
 }
+// Device functions of each source file, loaded eagerly when the first
+// context is created on a device (see preload_all_kernels in tof_api.cu).
+void preload_kernels_core();
+void preload_kernels_gmg();
+void preload_kernels_lobpcg();
+void preload_kernels_pcg();
+void preload_kernels_topopt();
 // Error message of calls without a context (returned by tof_last_error(NULL)).
 void set_global_error(const std::string& msg);
 
@@ -102,7 +109,10 @@ struct Ctx {
   // LOBPCG workspace (FP32 node4): 2 sets x 3 blocks (S, KS, MS) of 3*max_modes
   float* lw32 = nullptr;
   double* lw64 = nullptr;      // FP64 refinement: X, KX, MX of max_modes
-  double* gram = nullptr;      // [2][24*24] + small-eig outputs
+  double* gram = nullptr;      // [12][24*24]: modal 0-3, 6, 8-11; static 4, 5, 7
+  // basis and block size of the last full-basis ([X W P], 3 x block)
+  // in-loop Rayleigh-Ritz step, whose Gram matrices stay in slots 10 / 11
+  int lob_last_n = 0, lob_last_m = 0;
   double* gram_part = nullptr; // [gram blocks][24*24]
   int gram_blocks = 0;
   // Scratch of the modal family (LOBPCG, eigenvalue sensitivities, effective
@@ -186,6 +196,13 @@ int pcg_pipe32(Ctx& c, const double* b, float* d, int R, double rtol, int maxite
                int* status, cudaStream_t s);
 // FP32 standard PCG from x = 0 (x must be zeroed by the caller)
 int pcg_std32(Ctx& c, const double* b, float* x, int R, double rtol, int maxiter, cudaStream_t s);
+
+// Diagnostic single launches for kernel timing (tof_time_kernel): the
+// coarse-level stencil operator of multigrid level `level` in its smoothing
+// form on the static lane's level vectors; the Rayleigh-Ritz eigensolver on
+// the Gram matrices of the last full-basis LOBPCG step (slots 10 / 11).
+int mg_launch_level_op(Ctx& c, int level, int R, cudaStream_t s, long long* nodes);
+int lob_launch_rayleigh_ritz(Ctx& c, cudaStream_t s, int* n);
 
 // multigrid (tof_gmg.cu)
 int mg_create(Ctx& c, int maxR);

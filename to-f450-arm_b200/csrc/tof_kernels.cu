@@ -739,4 +739,23 @@ void launch_add_f32_to_f64(long long n, const float* d, double* x, cudaStream_t 
   count_launch();
 }
 
+// Load every kernel of this file now (CUDA loads device functions lazily,
+// at first use, and a first use in the middle of a solve stalls it).
+void preload_kernels_core() {
+  auto touch = [](auto f) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(f));
+  };
+  touch(k_factors); touch(k_diag);
+  touch(k_matvec<float, 1>); touch(k_matvec<float, 2>); touch(k_matvec<float, 4>); touch(k_matvec<float, 8>);
+  touch(k_matvec<double, 1>); touch(k_matvec<double, 2>); touch(k_matvec<double, 4>); touch(k_matvec<double, 8>);
+  touch(k_pack<float>); touch(k_pack<double>); touch(k_unpack<float>); touch(k_unpack<double>);
+  touch(k_gram_partial<float>); touch(k_gram_partial<double>); touch(k_gram_reduce);
+  touch(k_gram2_partial<float>); touch(k_gram2_partial_f64); touch(k_gram2_reduce);
+  touch(k_quadform<float>); touch(k_quadform<double>);
+  touch(k_convert<double, float>); touch(k_convert<float, double>); touch(k_convert<double, double>);
+  touch(k_convert<float, float>);
+  touch(k_axpy64); touch(k_add_f32); touch(k_abs64); touch(k_add_f32_to_f64);
+}
+
 }  // namespace tof

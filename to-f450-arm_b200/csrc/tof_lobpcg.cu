@@ -489,9 +489,10 @@ static inline T* vec(void* base, int j, long long vs) {
   return reinterpret_cast<T*>(base) + j * vs;
 }
 
-static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s) {
-  double* GK = c.gram;
-  double* GM = c.gram + 576;
+static int lob_small_eig(Ctx& c, int n, int m, double drop, cudaStream_t s, const double* GK = nullptr,
+                         const double* GM = nullptr) {
+  if (!GK) GK = c.gram;
+  if (!GM) GM = c.gram + 576;
   double* C = c.gram + 2 * 576;
   double* th = c.gram + 3 * 576;
   int* info = c.status_m;
@@ -755,6 +756,14 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     drop_p = false;
     ncols_at[it & 1] = ncols;
     launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s, c.gram_part_m);
+    // keep a full-basis problem for tof_time_kernel: the first one, then
+    // one every 16 iterations (a 9 KB copy), so it comes from the late,
+    // well-conditioned iterations that make up most of a solve
+    if (ncols == 3 * nb && (c.lob_last_n != ncols || (it & 15) == 15)) {
+      cudaMemcpyAsync(c.gram + 10 * 576, GK, sizeof(double) * 2 * 576, cudaMemcpyDeviceToDevice, s);
+      c.lob_last_n = ncols;
+      c.lob_last_m = nb;
+    }
     lob_small_eig(c, ncols, nb, drop, s);
     launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
                          (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
@@ -777,8 +786,9 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (!use_best) cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
   if (launch_matvec(c, 0, true, X6, KX6, nb, nullptr, s)) return -2;
   if (launch_matvec(c, 1, true, X6, MX6, nb, nullptr, s)) return -2;
-  launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, GK, GM, s, c.gram_part_m);
-  lob_small_eig(c, nb, nb, 1e-14, s);
+  // (its Gram matrices go to slots 8 / 9)
+  launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, c.gram + 8 * 576, c.gram + 9 * 576, s, c.gram_part_m);
+  lob_small_eig(c, nb, nb, 1e-14, s, c.gram + 8 * 576, c.gram + 9 * 576);
   // X64 = X6 C (first nmodes columns)
   {
     double* out = X64;
@@ -830,12 +840,28 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
 // Gram matrices and Rayleigh-Ritz) stalled at residual ~1 on the SIMP arm and
 // cantilever (the K X / M X recurrences drift by eps_32 * cond), so the mixed
 // mode puts FP32 where it is safe, in the multigrid preconditioner.
+int lob_launch_rayleigh_ritz(Ctx& c, cudaStream_t s, int* n) {
+  if (c.lob_last_n < 1) { c.last_error = "no LOBPCG iteration has run on this context"; return -1; }
+  *n = c.lob_last_n;
+  return lob_small_eig(c, c.lob_last_n, c.lob_last_m, 1e-12, s, c.gram + 10 * 576, c.gram + 11 * 576);
+}
+
 int lobpcg_run(Ctx& c, bool f64, int nmodes, int nb, double* X64, double* lam, double tol, int maxiter,
                int precond, int inner_iters, double inner_rtol, int* iters_out, double* resid_out, double* floor_out,
                cudaStream_t s) {
   if (!f64) precond = 2;
   return lobpcg_impl<double>(c, nmodes, nb, X64, lam, tol, maxiter, precond, inner_iters, inner_rtol, iters_out,
                              resid_out, floor_out, s);
+}
+
+// Load every kernel of this file now (CUDA loads device functions lazily,
+// at first use, and a first use in the middle of a solve stalls it).
+void preload_kernels_lobpcg() {
+  auto touch = [](auto f) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(f));
+  };
+  touch(k_add_scaled_cols); touch(k_lob_resid<double>); touch(k_small_eig); touch(k_lob_update<double>);
 }
 
 }  // namespace tof

@@ -686,4 +686,17 @@ int pcg_pipe32(Ctx& c, const double* b, float* d, int R, double rtol, int maxite
   return -1;
 }
 
+// Load every kernel of this file now (CUDA loads device functions lazily,
+// at first use, and a first use in the middle of a solve stalls it).
+void preload_kernels_pcg() {
+  auto touch = [](auto f) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(f));
+  };
+  touch(k_pcg_pipe<1>); touch(k_pcg_pipe<2>); touch(k_pcg_pipe<4>); touch(k_pcg_pipe<8>);
+  touch(k_pcg_plain<double, 1>); touch(k_pcg_plain<double, 2>); touch(k_pcg_plain<double, 4>);
+  touch(k_pcg_plain<double, 8>); touch(k_pcg_plain<float, 1>); touch(k_pcg_plain<float, 2>);
+  touch(k_pcg_plain<float, 4>); touch(k_pcg_plain<float, 8>); touch(k_barrier_selftest);
+}
+
 }  // namespace tof

@@ -222,4 +222,15 @@ void launch_eig_sens(int NE, const double* rho, const double* qK, const double* 
   count_launch();
 }
 
+// Load every kernel of this file now (CUDA loads device functions lazily,
+// at first use, and a first use in the middle of a solve stalls it).
+void preload_kernels_topopt() {
+  auto touch = [](auto f) {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(f));
+  };
+  touch(k_filter); touch(k_filter_den); touch(k_oc); touch(k_compliance_sens); touch(k_sum_partials);
+  touch(k_mass_quad); touch(k_eig_sens);
+}
+
 }  // namespace tof

@@ -28,6 +28,13 @@ class SolveStats(ctypes.Structure):
     _fields_ = [("status", c_int), ("iters", c_int), ("outer", c_int), ("relres", c_double), ("floor", c_double)]
 
 
+class KernelTiming(ctypes.Structure):
+    _fields_ = [("us", c_double), ("bytes", c_double), ("flops", c_double), ("units", c_longlong)]
+
+
+KERNEL_MATVEC_F32, KERNEL_MG_LEVEL_OP, KERNEL_RAYLEIGH_RITZ, KERNEL_VCYCLE = range(4)
+
+
 class SimpParams(ctypes.Structure):
     _fields_ = [("penal", c_double), ("emin", c_double), ("mass_threshold", c_double), ("mass_q", c_double)]
 
@@ -82,6 +89,7 @@ SIGNATURES = {
     "tof_mg_export": (c_int, [P, c_int, P, P]),
     "tof_mg_apply": (c_int, [P, P, P, c_int, P]),
     "tof_mg_setup": (c_int, [P, P]),
+    "tof_time_kernel": (c_int, [P, c_int, c_int, c_int, c_int, POINTER(KernelTiming), P]),
 }
 
 _lib = None
