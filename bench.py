@@ -113,7 +113,7 @@ def reference_arm(a, rank, world):
 class ClockSampler:
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_power_cap,utilization.gpu")
 
     def __init__(self, index):
         self.index = index
@@ -137,7 +137,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
             out, _ = self.proc.communicate()
-        sm, smax, reasons = [], 0.0, set()
+        sm, smax, reasons, busy = [], 0.0, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in out.strip().splitlines():
             parts = [p.strip() for p in ln.split(",")]
@@ -151,10 +151,17 @@ class ClockSampler:
             for nm, v in zip(names, parts[3:7]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+            if len(parts) > 7:
+                try:
+                    busy.append(float(parts[7]))
+                except ValueError:
+                    pass
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        if busy:   # nvidia-smi utilization.gpu: share of time a kernel was running
+            out["gpu_busy_mean_pct"] = statistics.mean(busy)
+        return out
 
 
 def l2_flush(buf):
