@@ -115,20 +115,27 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
 // |a_pq| <= kJacAbs ||A||_F, the rounding level of the rotations themselves
 // (the backward error of QR), which ends the iteration on the nearly
 // singular Gram matrices of the SVQB path.  The iteration ends at the first
-// round whose input matrix meets the criterion everywhere.  The four terms
-// of an element are summed as (t1 + (t2 + t3)) + t4 with t2, t3 exchanged
-// under i <-> j, so the matrix stays exactly symmetric.  The critical path
-// is one rotation, one element update and two barriers per round (~1 400
-// cycles measured on a B200, a dependent chain of shared loads and FP64
-// operations): 6-10 sweeps of K - 1 rounds on the graded Rayleigh-Ritz
-// matrices of LOBPCG, against one Givens rotation per step of the serial QR
-// bulge chase on one warp.
+// tested round whose input matrix meets the criterion everywhere.  A round
+// is one rotation (~530 cycles on a B200: two dependent FP64 reciprocal
+// square roots), a barrier, the element update of all 18 warps (~850
+// cycles) and a barrier: 6-10 sweeps of K - 1 rounds on the graded
+// Rayleigh-Ritz matrices of LOBPCG, against one Givens rotation per step of
+// the serial QR bulge chase on one warp.  Computing the next round's
+// rotations during the update (a spare warp, one barrier per round) was
+// measured no faster: the rotation chain then competes with the update for
+// issue slots.
 // On return d[k] / V[:, k] are the eigenpairs (unsorted); false if
-// kJacSweeps sweeps did not converge.  A is destroyed; A2 and V2 are scratch.
+// kJacSweeps sweeps did not converge.  S (the input) is left unchanged; the
+// iteration runs in JA / JV, two matrix buffers each, selected by the
+// round's parity (indexing one shared array rather than swapping pointers
+// keeps every access a shared-memory load).  The stopping test is evaluated
+// on every kJacTestEvery-th round's input (up to kJacTestEvery - 1 extra
+// rounds of rotations at the rounding level, for one test in four).
 // ---------------------------------------------------------------------------
 constexpr int LDA = kMaxBasis + 1;
 constexpr int kEigThreads = kMaxBasis * kMaxBasis;   // one thread per element
 constexpr int kJacSweeps = 40;
+constexpr int kJacTestEvery = 4;
 constexpr double kJacTol = 1e-14;
 constexpr double kJacAbs = 1e-15;
 
@@ -137,8 +144,8 @@ __device__ __forceinline__ bool jac_offdiag_live(double apq, double app, double 
   return a2 > kJacTol * kJacTol * fabs(app * aqq) && a2 > floor2;
 }
 
-__device__ bool cta_jacobi(double (*A)[LDA], double (*A2)[LDA], double (*V)[LDA], double (*V2)[LDA], double* d,
-                           int K) {
+__device__ bool cta_jacobi(const double (*S)[LDA], double (*JA)[kMaxBasis][LDA], double (*JV)[kMaxBasis][LDA],
+                           double (*V)[LDA], double* d, int K) {
   // per index x of the round: the new row x of J^T A is
   // jal[x] A[x, :] + jbe[x] A[jmt[x], :] (the same for the columns of A J)
   __shared__ double jal[kMaxBasis + 1], jbe[kMaxBasis + 1];
@@ -159,9 +166,13 @@ __device__ bool cta_jacobi(double (*A)[LDA], double (*A2)[LDA], double (*V)[LDA]
     jpq[r][k][0] = (unsigned char)min(p, q);
     jpq[r][k][1] = (unsigned char)max(p, q);
   }
-  const double a2 = warp_sum(own ? A[i][j] * A[i][j] : 0.0);   // ||A||_F^2
+  const double s0 = own ? S[i][j] : 0.0;
+  const double a2 = warp_sum(s0 * s0);   // ||A||_F^2
   if ((t & 31) == 0) red[t >> 5] = a2;
-  if (own) V[i][j] = (i == j) ? 1.0 : 0.0;
+  if (own) {
+    JA[0][i][j] = s0;
+    JV[0][i][j] = (i == j) ? 1.0 : 0.0;
+  }
   __syncthreads();
   if (t == 0) {
     double f = 0.0;
@@ -170,10 +181,7 @@ __device__ bool cta_jacobi(double (*A)[LDA], double (*A2)[LDA], double (*V)[LDA]
   }
   __syncthreads();
   const double floor2 = kJacAbs * kJacAbs * fro2;
-  double(*Ac)[LDA] = A;
-  double(*An)[LDA] = A2;
-  double(*Vc)[LDA] = V;
-  double(*Vn)[LDA] = V2;
+  int cur = 0;
   bool conv = M <= 0;
   for (int it = 0, r = 0; !conv && it < kJacSweeps * M; ++it, r = (r + 1 == M) ? 0 : r + 1) {
     if (t < NP / 2) {
@@ -181,7 +189,7 @@ __device__ bool cta_jacobi(double (*A)[LDA], double (*A2)[LDA], double (*V)[LDA]
       double c = 1.0, sn = 0.0;
       bool rot = false;
       if (q < K) {
-        const double app = Ac[p][p], aqq = Ac[q][q], apq = Ac[p][q];
+        const double app = JA[cur][p][p], aqq = JA[cur][q][q], apq = JA[cur][p][q];
         if (jac_offdiag_live(apq, app, aqq, floor2)) {
           // tan(2 phi) = 2 a_pq / (a_qq - a_pp), |phi| <= pi / 4:
           // c = (r + |d|) / sqrt(2 r (r + |d|)), s = sgn(d) e / sqrt(2 r (r + |d|))
@@ -199,34 +207,32 @@ __device__ bool cta_jacobi(double (*A)[LDA], double (*A2)[LDA], double (*V)[LDA]
       jal[q] = c; jbe[q] = sn;  jmt[q] = rot ? p : q;
     }
     __syncthreads();
-    bool bad = false;
+    // untested rounds count as unconverged
+    bool bad = it % kJacTestEvery != 0;
     if (own) {
+      const double aij = JA[cur][i][j];
+      if (!bad) bad = i != j && jac_offdiag_live(aij, JA[cur][i][i], JA[cur][j][j], floor2);
       const double ai = jal[i], bi = jbe[i], aj = jal[j], bj = jbe[j];
       const int mi = jmt[i], mj = jmt[j];
-      const double aij = Ac[i][j];
-      bad = i != j && jac_offdiag_live(aij, Ac[i][i], Ac[j][j], floor2);
       double v;
       if (mi == j && mi != i) {
         v = 0.0;                           // the rotated pair's off-diagonal
       } else {
         const double t1 = (ai * aj) * aij;
-        const double t2 = (ai * bj) * Ac[i][mj];
-        const double t3 = (bi * aj) * Ac[mi][j];
-        const double t4 = (bi * bj) * Ac[mi][mj];
+        const double t2 = (ai * bj) * JA[cur][i][mj];
+        const double t3 = (bi * aj) * JA[cur][mi][j];
+        const double t4 = (bi * bj) * JA[cur][mi][mj];
         v = (t1 + (t2 + t3)) + t4;
       }
-      An[i][j] = v;
-      Vn[i][j] = fma(bj, Vc[i][mj], aj * Vc[i][j]);
+      JA[cur ^ 1][i][j] = v;
+      JV[cur ^ 1][i][j] = fma(bj, JV[cur][i][mj], aj * JV[cur][i][j]);
     }
-    // the round's input already met the criterion: nothing was rotated
+    // a tested round's input already met the criterion: nothing was rotated
     conv = !__syncthreads_or(bad);
-    if (!conv) {
-      double(*tA)[LDA] = Ac; Ac = An; An = tA;
-      double(*tV)[LDA] = Vc; Vc = Vn; Vn = tV;
-    }
+    if (!conv) cur ^= 1;
   }
-  if (own && i == j) d[i] = Ac[i][i];
-  if (Vc != V && own) V[i][j] = Vc[i][j];
+  if (own && i == j) d[i] = JA[cur][i][i];
+  if (own) V[i][j] = JV[cur][i][j];
   __syncthreads();
   return conv;
 }
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
                                                           const double* __restrict__ GM, double drop_tol, double* C,
                                                           double* theta, int* info) {
   __shared__ double A[kMaxBasis][LDA], B[kMaxBasis][LDA], V[kMaxBasis][LDA], Z[kMaxBasis][LDA];
-  __shared__ double A2[kMaxBasis][LDA], V2[kMaxBasis][LDA];
+  __shared__ double JA[2][kMaxBasis][LDA], JV[2][kMaxBasis][LDA];   // Jacobi work buffers
   __shared__ double D[kMaxBasis], ev[kMaxBasis], idg[kMaxBasis];
   __shared__ int keep[kMaxBasis], order[kMaxBasis];
   __shared__ int kr;
@@ -341,7 +347,7 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
       B[i][j] = 0.5 * (GM[i * n + j] + GM[j * n + i]) * D[i] * D[j];
     }
     __syncthreads();
-    ok = cta_jacobi(B, A2, V, V2, ev, n);
+    ok = cta_jacobi(B, JA, JV, V, ev, n);
     if (tid == 0) {
       double bmax = 0.0;
       for (int i = 0; i < n; ++i) bmax = fmax(bmax, ev[i]);
@@ -377,7 +383,7 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
     }
     __syncthreads();
   }
-  ok = cta_jacobi(A, A2, V, V2, ev, K) && ok;
+  ok = cta_jacobi(A, JA, JV, V, ev, K) && ok;
   if (tid < K) {                                           // ascending order (ties by index)
     const double e = ev[tid];
     int rank = 0;
