@@ -149,6 +149,8 @@ void launch_diag(Ctx& c, cudaStream_t s);
 // op: 0 K, 1 M, 2 |K| (entrywise absolute values; FP64 only)
 int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, const void* b_residual,
                   cudaStream_t s);
+// yK = K x and yM = M x (with the tip lump) in one launch per chunk of <= 8
+int launch_matvec_km(Ctx& c, bool f64, const void* x, void* yK, void* yM, int nrhs, cudaStream_t s);
 int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* coef, bool prev,
                    int R, cudaStream_t s);
 void launch_pack(const Ctx& c, const double* src, long long ld, void* dst, bool f64, int nvec, cudaStream_t s);

@@ -238,6 +238,154 @@ int launch_matvec(Ctx& c, int op, bool f64, const void* x, void* y, int nrhs, co
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// K x and M x of the same R vectors in one launch (LOBPCG's block products):
+// one TMA halo load of x and both element-matrix block sets staged per CTA;
+// each thread forms its node's K row, stores it, then its M row (plus the
+// lumped tip mass).  The same per-operator arithmetic as k_matvec, so the
+// results are bit-identical to two k_matvec launches.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct MatvecKMArgs {
+  Grid g;
+  const T* fK;
+  const T* fM;
+  const T* kebK;
+  const T* kebM;
+  const uint8_t* fix;
+  const T* tip;
+  T* yK;
+  T* yM;
+  long long vstride;
+};
+
+template <typename T, int R>
+__global__ void __launch_bounds__(512) k_matvec_km(const __grid_constant__ CUtensorMap tmx, MatvecKMArgs<T> a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  using V4 = typename Vec4<T>::type;
+  const Grid& g = a.g;
+  const TileGeom tg = tile_geom(g, blockIdx.x);
+  const int nfe = tg.EX * tg.EY * tg.EZ;
+  T* sx = reinterpret_cast<T*>(smem_raw);
+  const unsigned hb = halo_bytes<T>(g, R);
+  T* sKeK = reinterpret_cast<T*>(smem_raw + hb);
+  T* sKeM = sKeK + kKeBlocksLen;
+  T* sfK = sKeM + kKeBlocksLen;
+  T* sfM = sfK + nfe;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + ((hb + sizeof(T) * (2 * kKeBlocksLen + 2 * nfe) + 15) & ~15u));
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_arrive_expect_tx(bar, hb);
+    tma_load_5d(sx, &tmx, 0, tg.i0 - 1, tg.j0 - 1, tg.k0 - 1, 0, bar);
+  }
+  load_ke_blocks(a.kebK, sKeK);
+  load_ke_blocks(a.kebM, sKeM);
+  load_factor_tile(g, tg, a.fK, sfK);
+  load_factor_tile(g, tg, a.fM, sfM);
+  __syncthreads();   // mbarrier initialised before anyone waits on it
+  if (!__syncthreads_and(mbar_wait(bar, 0))) return;
+  int tx, ty, tz, n;
+  const bool live = thread_node(g, tg, tx, ty, tz, n);
+  const uint8_t fx = live ? __ldg(a.fix + n) : uint8_t(0);
+  if (live) {
+    T acc[R][3];
+    stencil_node<T, R>(sx, tg, sfK, sKeK, tx, ty, tz, acc);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      V4 out;
+      out.x = (fx & 1) ? T(0) : acc[r][0];
+      out.y = (fx & 2) ? T(0) : acc[r][1];
+      out.z = (fx & 4) ? T(0) : acc[r][2];
+      out.w = T(0);
+      reinterpret_cast<V4*>(a.yK + r * a.vstride)[n] = out;
+    }
+  }
+  // the CTA barrier keeps the two products from being interleaved (which
+  // would double the live registers)
+  __syncthreads();
+  if (live) {
+    T acc[R][3];
+    stencil_node<T, R>(sx, tg, sfM, sKeM, tx, ty, tz, acc);
+    const V4 tp = reinterpret_cast<const V4*>(a.tip)[n];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const V4 xc = halo_center<T>(sx, tg, r, tx, ty, tz);
+      acc[r][0] = fma(tp.x, xc.x, acc[r][0]);
+      acc[r][1] = fma(tp.y, xc.y, acc[r][1]);
+      acc[r][2] = fma(tp.z, xc.z, acc[r][2]);
+      V4 out;
+      out.x = (fx & 1) ? T(0) : acc[r][0];
+      out.y = (fx & 2) ? T(0) : acc[r][1];
+      out.z = (fx & 4) ? T(0) : acc[r][2];
+      out.w = T(0);
+      reinterpret_cast<V4*>(a.yM + r * a.vstride)[n] = out;
+    }
+  }
+}
+
+template <typename T, int R>
+static int matvec_km_launch_t(Ctx& c, const void* x, void* yK, void* yM, cudaStream_t s) {
+  CUtensorMap tm;
+  std::string err;
+  constexpr bool f64 = sizeof(T) == 8;
+  if (!encode_node4_map(&tm, x, c.g, R, f64, &err)) {
+    c.last_error = err;
+    return -2;
+  }
+  MatvecKMArgs<T> a;
+  a.g = c.g;
+  a.fK = reinterpret_cast<const T*>(f64 ? (const void*)c.fK64 : (const void*)c.fK32);
+  a.fM = reinterpret_cast<const T*>(f64 ? (const void*)c.fM64 : (const void*)c.fM32);
+  a.kebK = reinterpret_cast<const T*>(f64 ? (const void*)c.keb64 : (const void*)c.keb32);
+  a.kebM = reinterpret_cast<const T*>(f64 ? (const void*)c.meb64 : (const void*)c.meb32);
+  a.fix = c.fix;
+  a.tip = reinterpret_cast<const T*>(f64 ? (const void*)c.tip64 : (const void*)c.tip32);
+  a.yK = reinterpret_cast<T*>(yK);
+  a.yM = reinterpret_cast<T*>(yM);
+  a.vstride = (long long)c.g.NN * 4;
+  const int nfe = (c.g.TX + 1) * (c.g.TY + 1) * (c.g.TZ + 1);
+  size_t smem = halo_bytes<T>(c.g, R) + sizeof(T) * (2 * kKeBlocksLen + 2 * nfe);
+  smem = ((smem + 15) & ~size_t(15)) + 16;
+  auto kern = k_matvec_km<T, R>;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<c.g.ntiles, c.g.TX * c.g.TY * c.g.TZ, smem, s>>>(tm, a);
+  count_launch();
+  return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// yK = K x, yM = M x for nrhs vectors (chunks of at most 8, as launch_matvec)
+int launch_matvec_km(Ctx& c, bool f64, const void* x, void* yK, void* yM, int nrhs, cudaStream_t s) {
+  const size_t esz = f64 ? 8 : 4;
+  const long long vbytes = (long long)c.g.NN * 4 * esz;
+  int done = 0;
+  while (done < nrhs) {
+    int R = nrhs - done;
+    R = R >= 8 ? 8 : R >= 4 ? 4 : R >= 2 ? 2 : 1;
+    const char* xp = (const char*)x + done * vbytes;
+    char* kp = (char*)yK + done * vbytes;
+    char* mp = (char*)yM + done * vbytes;
+    int rc;
+    if (f64) {
+      switch (R) {
+        case 8: rc = matvec_km_launch_t<double, 8>(c, xp, kp, mp, s); break;
+        case 4: rc = matvec_km_launch_t<double, 4>(c, xp, kp, mp, s); break;
+        case 2: rc = matvec_km_launch_t<double, 2>(c, xp, kp, mp, s); break;
+        default: rc = matvec_km_launch_t<double, 1>(c, xp, kp, mp, s); break;
+      }
+    } else {
+      switch (R) {
+        case 8: rc = matvec_km_launch_t<float, 8>(c, xp, kp, mp, s); break;
+        case 4: rc = matvec_km_launch_t<float, 4>(c, xp, kp, mp, s); break;
+        case 2: rc = matvec_km_launch_t<float, 2>(c, xp, kp, mp, s); break;
+        default: rc = matvec_km_launch_t<float, 1>(c, xp, kp, mp, s); break;
+      }
+    }
+    if (rc) return rc;
+    done += R;
+  }
+  return 0;
+}
+
 // y = sx x + sp y_prev + sr D^-1 (b - K x) on the fine level, FP32, R in
 // {1,2,4,8}; coef = device (sx, sp, sr), y_prev read only with prev
 int launch_smooth0(Ctx& c, const float* x, float* y, const float* b, const float* dinv, const float* coef, bool prev,
@@ -749,6 +897,9 @@ void preload_kernels_core() {
   touch(k_factors); touch(k_diag);
   touch(k_matvec<float, 1>); touch(k_matvec<float, 2>); touch(k_matvec<float, 4>); touch(k_matvec<float, 8>);
   touch(k_matvec<double, 1>); touch(k_matvec<double, 2>); touch(k_matvec<double, 4>); touch(k_matvec<double, 8>);
+  touch(k_matvec_km<double, 1>); touch(k_matvec_km<double, 2>); touch(k_matvec_km<double, 4>);
+  touch(k_matvec_km<double, 8>); touch(k_matvec_km<float, 1>); touch(k_matvec_km<float, 2>);
+  touch(k_matvec_km<float, 4>); touch(k_matvec_km<float, 8>);
   touch(k_pack<float>); touch(k_pack<double>); touch(k_unpack<float>); touch(k_unpack<double>);
   touch(k_gram_partial<float>); touch(k_gram_partial<double>); touch(k_gram_reduce);
   touch(k_gram2_partial<float>); touch(k_gram2_partial_f64); touch(k_gram2_reduce);

@@ -276,17 +276,6 @@ __device__ void cta_forward(double (*T)[LDA], double (*B)[LDA], const double* id
   __syncthreads();
 }
 
-// T <- L^-T T (backward substitution, n x nc); one barrier per row.
-__device__ void cta_backward(double (*T)[LDA], double (*B)[LDA], const double* idiag, int n, int nc) {
-  const int t = threadIdx.x, i = t / kMaxBasis, j = t % kMaxBasis;
-  for (int l = n - 1; l > 0; --l) {
-    if (i < l && j < nc) T[i][j] = fma(-B[l][i] * idiag[l], T[l][j], T[i][j]);
-    __syncthreads();
-  }
-  if (i < n && j < nc) T[i][j] *= idiag[i];
-  __syncthreads();
-}
-
 // Rayleigh-Ritz: the m smallest eigenpairs of G_K c = theta G_M c (n x n).
 // Both Grams are scaled by D = diag(G_M)^-1/2.  Fast path: Cholesky
 // D G_M D = L L^T (pivots above kCholPivot, i.e. a well-conditioned basis)
@@ -332,14 +321,28 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
   bool ok = true;
   int K = n;
   if (chol) {
-    // A <- L^-1 A, then Z <- L^-1 A^T = (L^-1 A_0 L^-T)^T, symmetrised into A
+    // Z <- L^-1 (forward substitution on the identity, one barrier per row),
+    // then A <- L^-1 A L^-T as two dense products of one step each; thread
+    // (i, j) forms element (i, j) and element (j, i) of V L^-T in the same
+    // order and stores their mean, so A stays exactly symmetric.  Z is kept
+    // for the back-transformation of the eigenvectors (one more product).
     const int ti = tid / kMaxBasis, tj = tid % kMaxBasis;
     const bool te = ti < n && tj < n;
-    cta_forward(A, B, idg, n, n);
-    if (te) Z[tj][ti] = A[ti][tj];
+    if (te) Z[ti][tj] = ti == tj ? 1.0 : 0.0;
     __syncthreads();
     cta_forward(Z, B, idg, n, n);
-    if (te) A[ti][tj] = 0.5 * (Z[ti][tj] + Z[tj][ti]);
+    if (te) {                                              // V = L^-1 A
+      double acc = 0.0;
+      for (int k = 0; k <= ti; ++k) acc = fma(Z[ti][k], A[k][tj], acc);
+      V[ti][tj] = acc;
+    }
+    __syncthreads();
+    if (te) {
+      double a1 = 0.0, a2 = 0.0;
+      for (int k = 0; k <= tj; ++k) a1 = fma(V[ti][k], Z[tj][k], a1);
+      for (int k = 0; k <= ti; ++k) a2 = fma(V[tj][k], Z[ti][k], a2);
+      A[ti][tj] = 0.5 * (a1 + a2);
+    }
     __syncthreads();
   } else {
     for (int w = tid; w < n * n; w += blockDim.x) {       // B was overwritten by the failed Cholesky
@@ -395,13 +398,12 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
   if (K < m || !ok) return;
   if (tid < m) theta[tid] = ev[order[tid]];
   if (chol) {
-    // C = D L^-T U[:, order[:m]]
-    for (int w = tid; w < n * m; w += blockDim.x) Z[w / m][w % m] = V[w / m][order[w % m]];
-    __syncthreads();
-    cta_backward(Z, B, idg, n, m);
+    // C = D L^-T U[:, order[:m]] (Z holds L^-1, lower triangular)
     for (int w = tid; w < n * m; w += blockDim.x) {
-      const int i = w / m, k = w % m;
-      C[i * m + k] = D[i] * Z[i][k];
+      const int i = w / m, k = w % m, col = order[k];
+      double acc = 0.0;
+      for (int l = i; l < n; ++l) acc = fma(Z[l][i], V[l][col], acc);
+      C[i * m + k] = D[i] * acc;
     }
   } else {
     for (int w = tid; w < n * m; w += blockDim.x) {        // C = D Z U[:, order[:m]]
@@ -540,8 +542,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   if (precond == 2 && mg_ensure(c, s)) return -2;
   // X <- X64 (first nb vectors), KX, MX
   launch_convert(X64, true, B.S[cur], f64, (long long)nb * vs, s);
-  if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
-  if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
+  if (launch_matvec_km(c, f64, B.S[cur], B.KS[cur], B.MS[cur], nb, s)) return -2;
   // initial Rayleigh-Ritz on X alone
   launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], identity_cols(), nb, GK, GM, s, c.gram_part_m);
   lob_small_eig(c, nb, nb, drop, s);
@@ -565,11 +566,9 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   // (and before convergence is accepted) bounds that drift.
   auto refresh = [&]() -> int {
     void* S = B.S[cur];
-    if (launch_matvec(c, 0, f64, S, B.KS[cur], nb, nullptr, s)) return -2;
-    if (launch_matvec(c, 1, f64, S, B.MS[cur], nb, nullptr, s)) return -2;
+    if (launch_matvec_km(c, f64, S, B.KS[cur], B.MS[cur], nb, s)) return -2;
     const T* P = vec<T>(S, 2 * nb, vs);
-    if (launch_matvec(c, 0, f64, P, vec<T>(B.KS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
-    if (launch_matvec(c, 1, f64, P, vec<T>(B.MS[cur], 2 * nb, vs), nb, nullptr, s)) return -2;
+    if (launch_matvec_km(c, f64, P, vec<T>(B.KS[cur], 2 * nb, vs), vec<T>(B.MS[cur], 2 * nb, vs), nb, s)) return -2;
     return 0;
   };
   // Soft locking (as scipy.sparse.linalg.lobpcg's active mask): a wanted
@@ -658,8 +657,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       // iterate with fresh products and without P
       ++restarts;
       cudaMemcpyAsync(B.S[cur], X6, sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
-      if (launch_matvec(c, 0, f64, B.S[cur], B.KS[cur], nb, nullptr, s)) return -2;
-      if (launch_matvec(c, 1, f64, B.S[cur], B.MS[cur], nb, nullptr, s)) return -2;
+      if (launch_matvec_km(c, f64, B.S[cur], B.KS[cur], B.MS[cur], nb, s)) return -2;
       for (int j = 0; j < nmodes; ++j) locked[j] = false;
       drop_p = true;
     } else if (best < kLobNearFloor &&
@@ -749,8 +747,10 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       if (pcg_std32(c, b64, d32, R, inner_rtol, inner_iters, s)) return -2;
       launch_convert(d32, false, W, f64, (long long)na * vs, s);
     }
-    if (launch_matvec(c, 0, f64, W, vec<T>(B.KS[cur], nb, vs), na, nullptr, s)) return -2;
-    if (launch_matvec(c, 1, f64, W, vec<T>(B.MS[cur], nb, vs), na, nullptr, s)) return -2;
+    // K W, M W: one launch for the R >= na vectors when they stay inside the
+    // W block (the columns beyond na are never read)
+    if (launch_matvec_km(c, f64, W, vec<T>(B.KS[cur], nb, vs), vec<T>(B.MS[cur], nb, vs), R <= nb ? R : na, s))
+      return -2;
     // basis [X, W_active, P_active]
     ColMap cols;
     int ncols = 0;
@@ -790,8 +790,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   double* KX6 = c.lw64 + (long long)c.max_modes * vs;
   double* MX6 = c.lw64 + 2LL * c.max_modes * vs;
   if (!use_best) cudaMemcpyAsync(X6, B.S[cur], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
-  if (launch_matvec(c, 0, true, X6, KX6, nb, nullptr, s)) return -2;
-  if (launch_matvec(c, 1, true, X6, MX6, nb, nullptr, s)) return -2;
+  if (launch_matvec_km(c, true, X6, KX6, MX6, nb, s)) return -2;
   // (its Gram matrices go to slots 8 / 9)
   launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, c.gram + 8 * 576, c.gram + 9 * 576, s, c.gram_part_m);
   lob_small_eig(c, nb, nb, 1e-14, s, c.gram + 8 * 576, c.gram + 9 * 576);
