@@ -70,7 +70,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs, const T* __restrict__ KX,
                                                    const T* __restrict__ MX, const double* __restrict__ theta,
                                                    const T* __restrict__ dinv, T* S, ColMap wslot, double* part,
-                                                   unsigned* counter, double* out) {
+                                                   unsigned* counter, double* out, float* w32, int na, int R32) {
   using V4 = typename Vec4<T>::type;
   __shared__ double red[16 * 32];
   double v[16];
@@ -91,8 +91,15 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
       v[2 * j] += double(w.x) * w.x + double(w.y) * w.y + double(w.z) * w.z;
       v[2 * j + 1] += double(kx.x) * kx.x + double(kx.y) * kx.y + double(kx.z) * kx.z;
       if (dinv) { w.x *= di.x; w.y *= di.y; w.z *= di.z; }
-      if (wslot.col[j] >= 0) reinterpret_cast<V4*>(S + wslot.col[j] * vs)[n] = w;
+      if (wslot.col[j] >= 0) {
+        reinterpret_cast<V4*>(S + wslot.col[j] * vs)[n] = w;
+        if (w32)
+          reinterpret_cast<float4*>(w32 + (wslot.col[j] - nb) * vs)[n] =
+              make_float4(float(w.x), float(w.y), float(w.z), 0.f);
+      }
     }
+    if (w32)
+      for (int k = na; k < R32; ++k) reinterpret_cast<float4*>(w32 + k * vs)[n] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   double tot[16];
   if (last_block<16>(v, part, counter, red, tot) && threadIdx.x == 0) {
@@ -599,11 +606,19 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   // observed.  Slots 0 / 1 alternate; slot 2 is for synchronous reads.
   struct LobSlot { double r[16]; double th[8]; int info; int pad; };
   LobSlot* hp = reinterpret_cast<LobSlot*>(c.lob_pin);
+  // with the single-V-cycle preconditioner the residual kernel also writes
+  // the multigrid right-hand sides (FP32 W of the active columns, zero
+  // padding up to the cycle's block size)
+  const bool w32_out = precond == 2 && inner_iters <= 1;
   auto launch_resid = [&](int slot) {
     const T* dinv = nullptr;
     if (precond == 0) dinv = f64 ? (const T*)c.dinvK64 : (const T*)c.dinvK32;
+    int na_now = 0;
+    for (int j = 0; j < nb; ++j) na_now += wslot.col[j] >= 0 ? 1 : 0;
+    const int R32 = na_now <= 1 ? 1 : na_now <= 2 ? 2 : na_now <= 4 ? 4 : 8;
     k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, (T*)B.S[cur],
-                                           wslot, c.gram_part_m, c.counters_m, rn);
+                                           wslot, c.gram_part_m, c.counters_m, rn,
+                                           w32_out ? mg_rhs(c, 1) : nullptr, na_now, R32);
     count_launch();
     cudaMemcpyAsync(hp[slot].r, rn, sizeof(hp[slot].r), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(hp[slot].th, th, sizeof(hp[slot].th), cudaMemcpyDeviceToHost, s);
@@ -710,10 +725,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     const int R = na <= 1 ? 1 : na <= 2 ? 2 : na <= 4 ? 4 : 8;
     if (precond == 2 && inner_iters <= 1) {
       // W <- V-cycle(W): the FP32 multigrid approximation of K^-1
+      // (the right-hand sides were written by the residual kernel)
       if (mg_ensure(c, s)) return -2;
-      float* r32 = mg_rhs(c, 1);
-      if (R > na) cudaMemsetAsync(r32, 0, sizeof(float) * R * vs, s);
-      launch_convert(W, f64, r32, false, (long long)na * vs, s);
       if (mg_vcycle(c, R, s, 1)) return -2;
       launch_convert(mg_out(c, 1), false, W, f64, (long long)na * vs, s);
     } else if (precond == 2) {
