@@ -286,7 +286,8 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(dalloc(c, &c.gram_part, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.gram_part_m, (size_t)c.gram_blocks * 1152));
   A(dalloc(c, &c.counters_m, 16)); A(dalloc(c, &c.status_m, 16)); A(dalloc(c, &c.scal_m, 256));
-  A(cudaHostAlloc(&c.lob_pin, 3 * 256, cudaHostAllocDefault));
+  A(cudaHostAlloc(&c.lob_pin, 3 * 256, cudaHostAllocMapped));
+  if (c.lob_pin) A(cudaHostGetDevicePointer(&c.lob_pin_dev, c.lob_pin, 0));
   for (cudaEvent_t& ev : c.lob_ev) A(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
   if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error.str());

@@ -124,9 +124,11 @@ struct Ctx {
   unsigned* counters_m = nullptr; // [16]
   int* status_m = nullptr;       // [16]
   double* scal_m = nullptr;      // [256]
-  // LOBPCG: pinned host slots for the residual norms read one iteration
-  // late, and the events that mark them complete
-  void* lob_pin = nullptr;       // 3 slots of 256 bytes (cudaHostAlloc)
+  // LOBPCG: pinned, mapped host slots for the residual norms read one
+  // iteration late (written by the residual kernel through lob_pin_dev), and
+  // the events that mark them complete
+  void* lob_pin = nullptr;       // 3 slots of 256 bytes (cudaHostAlloc, mapped)
+  void* lob_pin_dev = nullptr;
   cudaEvent_t lob_ev[3] = {nullptr, nullptr, nullptr};
 
   // persistent-launch capacity for each kernel flavour

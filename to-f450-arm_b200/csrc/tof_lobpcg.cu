@@ -44,6 +44,9 @@ constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M
 constexpr int kLobStall = 500;
 constexpr double kLobDiverge = 1e3;
 constexpr double kLobNearFloor = 1e-3;
+// The best iterate is copied aside only below this residual (at or above
+// kLobNearFloor, where it is restarted from or returned; and at maxiter).
+constexpr double kLobKeepBelow = 1e-2;
 // Before stopping, a residual kLobRestartGrowth times above the best
 // iterate's restarts the iteration from that iterate without P (at most
 // kLobMaxRestarts times).
@@ -66,11 +69,22 @@ __global__ void k_add_scaled_cols(long long n, int nv, const double* __restrict_
 // column), and the norms ||W_j||^2, ||KX_j||^2 (unscaled residual) of every
 // column, reduced by the last CTA into out[2j], out[2j+1]
 // ---------------------------------------------------------------------------
+// What the host reads of each LOBPCG iteration (pinned, mapped host memory
+// written by the residual kernel): the residual and K X norms of each
+// column, theta, and the rank word of the Rayleigh-Ritz step before it.
+struct LobSlot {
+  double r[16];
+  double th[8];
+  int info;
+  int pad;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs, const T* __restrict__ KX,
                                                    const T* __restrict__ MX, const double* __restrict__ theta,
                                                    const T* __restrict__ dinv, T* S, ColMap wslot, double* part,
-                                                   unsigned* counter, double* out, float* w32, int na, int R32) {
+                                                   unsigned* counter, double* out, float* w32, int na, int R32,
+                                                   const int* info, LobSlot* host) {
   using V4 = typename Vec4<T>::type;
   __shared__ double red[16 * 32];
   double v[16];
@@ -105,6 +119,13 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
   if (last_block<16>(v, part, counter, red, tot) && threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) out[k] = tot[k];
+    if (host) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) host->r[k] = tot[k];
+      for (int j = 0; j < nb; ++j) host->th[j] = theta[j];
+      host->info = *info;
+      __threadfence_system();
+    }
   }
 }
 
@@ -604,8 +625,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   // queued work and the host never drains the stream.  Locking, restart and
   // stopping decisions therefore act one iteration later than they were
   // observed.  Slots 0 / 1 alternate; slot 2 is for synchronous reads.
-  struct LobSlot { double r[16]; double th[8]; int info; int pad; };
   LobSlot* hp = reinterpret_cast<LobSlot*>(c.lob_pin);
+  LobSlot* hp_dev = reinterpret_cast<LobSlot*>(c.lob_pin_dev);
   // with the single-V-cycle preconditioner the residual kernel also writes
   // the multigrid right-hand sides (FP32 W of the active columns, zero
   // padding up to the cycle's block size)
@@ -618,11 +639,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     const int R32 = na_now <= 1 ? 1 : na_now <= 2 ? 2 : na_now <= 4 ? 4 : 8;
     k_lob_resid<T><<<rblocks, 256, 0, s>>>(NN, nb, vs, (T*)B.KS[cur], (T*)B.MS[cur], th, dinv, (T*)B.S[cur],
                                            wslot, c.gram_part_m, c.counters_m, rn,
-                                           w32_out ? mg_rhs(c, 1) : nullptr, na_now, R32);
+                                           w32_out ? mg_rhs(c, 1) : nullptr, na_now, R32, info, hp_dev + slot);
     count_launch();
-    cudaMemcpyAsync(hp[slot].r, rn, sizeof(hp[slot].r), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(hp[slot].th, th, sizeof(hp[slot].th), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&hp[slot].info, info, sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaEventRecord(c.lob_ev[slot], s);
   };
   auto read_resid = [&](int slot) -> int {
@@ -649,6 +667,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   double best_res[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int it_best = 0;
   bool use_best = false;
+  bool have_best = false;                      // X6 holds the best iterate
   double* X6 = c.lw64;                         // holds the best iterate (free until the final step)
   int pending = -1;                            // slot of a residual launched but not yet read
   // Bookkeeping on the residual of the iterate before the current one (in
@@ -666,7 +685,12 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       best = worst;
       it_best = itk;
       for (int j = 0; j < nmodes; ++j) best_res[j] = rres[j];
-      cudaMemcpyAsync(X6, B.S[cur ^ 1], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+      // the iterate itself is kept only once it could be returned or
+      // restarted from (a 5.5 MB copy on the 2 mm arm)
+      if (worst < kLobKeepBelow) {
+        cudaMemcpyAsync(X6, B.S[cur ^ 1], sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
+        have_best = true;
+      }
     } else if (best < kLobNearFloor && worst > kLobRestartGrowth * best && restarts < kLobMaxRestarts) {
       // the residual grew well past the best iterate: continue from the best
       // iterate with fresh products and without P
@@ -795,7 +819,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (o < 0) return o;
   }
   if (iters_out) *iters_out = it;
-  if (!conv && it >= maxiter && worst > best) use_best = true;
+  if (!conv && it >= maxiter && worst > best && have_best) use_best = true;
   if (use_best && resid_out)
     for (int j = 0; j < nmodes; ++j) resid_out[j] = best_res[j];
   // final FP64 Rayleigh-Ritz on fresh FP64 products of X6 (the best iterate,
