@@ -79,6 +79,9 @@ struct LobSlot {
   int pad;
 };
 
+// One work item per (node, column): the residual column j of node n, its
+// norms accumulated per thread and reduced by the last block; items
+// nb .. nb + (R32 - na) - 1 zero the multigrid padding vectors na .. R32-1.
 template <typename T>
 __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs, const T* __restrict__ KX,
                                                    const T* __restrict__ MX, const double* __restrict__ theta,
@@ -90,30 +93,39 @@ __global__ void __launch_bounds__(256) k_lob_resid(int NN, int nb, long long vs,
   double v[16];
 #pragma unroll
   for (int k = 0; k < 16; ++k) v[k] = 0.0;
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
-    V4 di;
-    if (dinv) di = reinterpret_cast<const V4*>(dinv)[n];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (j >= nb) break;
-      const size_t o = j * vs / 4 + n;
-      const V4 kx = reinterpret_cast<const V4*>(KX)[o];
-      const V4 mx = reinterpret_cast<const V4*>(MX)[o];
-      const T th = T(theta[j]);
-      V4 w;
-      w.x = kx.x - th * mx.x; w.y = kx.y - th * mx.y; w.z = kx.z - th * mx.z; w.w = T(0);
-      v[2 * j] += double(w.x) * w.x + double(w.y) * w.y + double(w.z) * w.z;
-      v[2 * j + 1] += double(kx.x) * kx.x + double(kx.y) * kx.y + double(kx.z) * kx.z;
-      if (dinv) { w.x *= di.x; w.y *= di.y; w.z *= di.z; }
-      if (wslot.col[j] >= 0) {
-        reinterpret_cast<V4*>(S + wslot.col[j] * vs)[n] = w;
-        if (w32)
-          reinterpret_cast<float4*>(w32 + (wslot.col[j] - nb) * vs)[n] =
-              make_float4(float(w.x), float(w.y), float(w.z), 0.f);
-      }
+  const int npad = w32 ? R32 - na : 0;
+  const long long items = (long long)NN * (nb + npad);
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < items;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int j = int(idx / NN), n = int(idx % NN);
+    if (j >= nb) {
+      reinterpret_cast<float4*>(w32 + (na + j - nb) * vs)[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+      continue;
     }
-    if (w32)
-      for (int k = na; k < R32; ++k) reinterpret_cast<float4*>(w32 + k * vs)[n] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const size_t o = j * vs / 4 + n;
+    const V4 kx = reinterpret_cast<const V4*>(KX)[o];
+    const V4 mx = reinterpret_cast<const V4*>(MX)[o];
+    const T th = T(theta[j]);
+    V4 w;
+    w.x = kx.x - th * mx.x; w.y = kx.y - th * mx.y; w.z = kx.z - th * mx.z; w.w = T(0);
+    const double rr = double(w.x) * w.x + double(w.y) * w.y + double(w.z) * w.z;
+    const double kk = double(kx.x) * kx.x + double(kx.y) * kx.y + double(kx.z) * kx.z;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k == j) { v[2 * k] += rr; v[2 * k + 1] += kk; }
+    if (dinv) {
+      const V4 di = reinterpret_cast<const V4*>(dinv)[n];
+      w.x *= di.x; w.y *= di.y; w.z *= di.z;
+    }
+    int ws = -1;                     // wslot.col[j] without a dynamic index into the parameter
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k == j) ws = wslot.col[k];
+    if (ws >= 0) {
+      reinterpret_cast<V4*>(S + ws * vs)[n] = w;
+      if (w32)
+        reinterpret_cast<float4*>(w32 + (ws - nb) * vs)[n] = make_float4(float(w.x), float(w.y), float(w.z), 0.f);
+    }
   }
   double tot[16];
   if (last_block<16>(v, part, counter, red, tot) && threadIdx.x == 0) {
@@ -447,9 +459,12 @@ __global__ void __launch_bounds__(kEigThreads) k_small_eig(int n, int m, const d
 // ---------------------------------------------------------------------------
 // block update: Xn = S C, Pn = S[:, nb:] C[nb:, :] for S, KS, MS
 // ---------------------------------------------------------------------------
-// One thread per (node, block in {S, KS, MS}): the ncols input node records
-// stream in as whole (coalesced) 4-component loads; the 2 nb outputs
-// accumulate in registers and are stored with a zero 4th component.
+// One thread per (node, block in {S, KS, MS}, output half): the X half
+// accumulates all ncols input columns, the P half the columns from nb on
+// (two threads with nb accumulators each rather than one with 2 nb: half
+// the registers, twice the threads in flight); the input node records
+// stream in as whole (coalesced) 4-component loads, the outputs are stored
+// with a zero 4th component.
 template <typename T>
 __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, ColMap cols, long long vs,
                                                     const T* __restrict__ S, const T* __restrict__ KS,
@@ -460,40 +475,38 @@ __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, C
   for (int i = threadIdx.x; i < ncols * nb; i += blockDim.x) sC[i] = T(C[i]);
   __syncthreads();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= 3LL * NN) return;
+  if (t >= 6LL * NN) return;
   const int n = int(t % NN);
-  const int b = int(t / NN);
+  const int b = int((t / NN) % 3);
+  const int half = int(t / (3LL * NN));      // 0: X = S C, 1: P = S[:, nb:] C[nb:, :]
   const T* src = b == 0 ? S : b == 1 ? KS : MS;
   T* dst = b == 0 ? S2 : b == 1 ? KS2 : MS2;
-  T x[8][3], p[8][3];
+  const int j0 = half ? nb : 0;
+  T x[8][3];
 #pragma unroll
   for (int k = 0; k < 8; ++k)
 #pragma unroll
-    for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = T(0);
+    for (int c = 0; c < 3; ++c) x[k][c] = T(0);
 #pragma unroll
   for (int j = 0; j < kMaxBasis; ++j) {
-    if (j < ncols) {
+    if (j >= j0 && j < ncols) {
       const V4 v = reinterpret_cast<const V4*>(src + cols.col[j] * vs)[n];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
         if (k < nb) {
           const T cf = sC[j * nb + k];
           x[k][0] = fma(cf, v.x, x[k][0]); x[k][1] = fma(cf, v.y, x[k][1]); x[k][2] = fma(cf, v.z, x[k][2]);
-          if (j >= nb) {
-            p[k][0] = fma(cf, v.x, p[k][0]); p[k][1] = fma(cf, v.y, p[k][1]); p[k][2] = fma(cf, v.z, p[k][2]);
-          }
         }
       }
     }
   }
+  T* out = dst + (half ? 2 * nb : 0) * vs;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     if (k < nb) {
-      V4 o, q;
+      V4 o;
       o.x = x[k][0]; o.y = x[k][1]; o.z = x[k][2]; o.w = T(0);
-      q.x = p[k][0]; q.y = p[k][1]; q.z = p[k][2]; q.w = T(0);
-      reinterpret_cast<V4*>(dst + k * vs)[n] = o;
-      reinterpret_cast<V4*>(dst + (2 * nb + k) * vs)[n] = q;
+      reinterpret_cast<V4*>(out + k * vs)[n] = o;
     }
   }
 }
@@ -501,7 +514,7 @@ __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, C
 template <typename T>
 static void launch_lob_update(int NN, int nb, int ncols, const ColMap& cols, long long vs, const T* S, const T* KS,
                               const T* MS, const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s) {
-  k_lob_update<T><<<int((3LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2);
+  k_lob_update<T><<<int((6LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2);
   count_launch();
 }
 
