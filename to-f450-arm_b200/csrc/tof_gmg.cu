@@ -359,6 +359,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(int nx, int ny, int nz
   double* Dg = sh;                     // [kCholB][LD] diagonal block
   double* Pn = sh + kCholB * LD;       // [rows below][LD] panel
   __shared__ int s_bad;
+  __shared__ double Rd[kCholB];
   if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
   for (int kb = 0; kb < n; kb += kCholB) {
@@ -389,8 +390,13 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(int nx, int ny, int nz
         A[(size_t)(kb + r0) * n + kb + c0] = Dg[r0 * LD + c0];
         A[(size_t)(kb + c0) * n + kb + r0] = Dg[r0 * LD + c0];
       }
-      if (c0 == r0) Y[kb + r0] = 1.0 / Dg[r0 * LD + r0];
+      if (c0 == r0) {
+        const double rd = 1.0 / Dg[r0 * LD + r0];
+        Y[kb + r0] = rd;
+        Rd[r0] = rd;
+      }
     }
+    __syncthreads();
     const int base = kb + w;
     for (int i = base + threadIdx.x; i < n; i += blockDim.x) {
       double x[kCholB];
@@ -401,7 +407,7 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_setup(int nx, int ny, int nz
         if (t < w) {
 #pragma unroll
           for (int u = 0; u < t; ++u) x[t] = fma(-x[u], Dg[t * LD + u], x[t]);
-          x[t] /= Dg[t * LD + t];
+          x[t] *= Rd[t];                          // (the pivots' reciprocals, formed once per panel)
           A[(size_t)i * n + kb + t] = x[t];
           A[(size_t)(kb + t) * n + i] = x[t];      // L^T in the upper triangle
           Pn[(i - base) * LD + t] = x[t];
@@ -444,34 +450,63 @@ __global__ void __launch_bounds__(256) k_mg_coarse_inverse(int n, const double* 
   double y[kInvSlots];
 #pragma unroll
   for (int m = 0; m < kInvSlots; ++m) y[m] = (lane + 32 * m == j) ? 1.0 : 0.0;
+  // Each step's row of L^T (forward) or L (backward) does not depend on y:
+  // it is loaded one step ahead (into cur / nxt), so the L2 latency overlaps
+  // the previous step's shuffle and updates instead of adding to every step.
+  // The updates are selects, not branches, which keeps y in registers (with
+  // branches the compiler placed it in local memory).
+  double cur[kInvSlots], nxt[kInvSlots];
+#pragma unroll
+  for (int m = 0; m < kInvSlots; ++m) {
+    const int i = lane + 32 * m;
+    cur[m] = i < n ? LLt[(size_t)j * n + i] : 0.0;
+    nxt[m] = 0.0;
+  }
   // forward: for k = j .. n-1: y_k /= L_kk; y_i -= L_ik y_k (i > k)
   for (int k = j; k < n; ++k) {
-    double own = 0.0;
-#pragma unroll
-    for (int m = 0; m < kInvSlots; ++m)
-      if (m == (k >> 5)) own = y[m];
-    const double yk = __shfl_sync(0xffffffffu, own, k & 31) * idg[k];
-    const double* col = LLt + (size_t)k * n;          // L^T row k = L column k
+    const int kn = k + 1 < n ? k + 1 : k;
 #pragma unroll
     for (int m = 0; m < kInvSlots; ++m) {
       const int i = lane + 32 * m;
-      if (i == k) y[m] = yk;
-      else if (i > k && i < n) y[m] = fma(-col[i], yk, y[m]);
+      nxt[m] = i < n ? LLt[(size_t)kn * n + i] : 0.0;
+    }
+    const int km = k >> 5;
+    double own = 0.0;
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m) own = m == km ? y[m] : own;
+    const double yk = __shfl_sync(0xffffffffu, own, k & 31) * idg[k];
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m) {
+      const int i = lane + 32 * m;
+      const double upd = fma(-((i > k && i < n) ? cur[m] : 0.0), yk, y[m]);
+      y[m] = i == k ? yk : upd;
+      cur[m] = nxt[m];
     }
   }
   // backward: for k = n-1 .. 0: x_k = y_k / L_kk; y_i -= L_ki x_k (i < k)
-  for (int k = n - 1; k >= 0; --k) {
-    double own = 0.0;
 #pragma unroll
-    for (int m = 0; m < kInvSlots; ++m)
-      if (m == (k >> 5)) own = y[m];
-    const double xk = __shfl_sync(0xffffffffu, own, k & 31) * idg[k];
-    const double* row = LLt + (size_t)k * n;          // L row k (lower part)
+  for (int m = 0; m < kInvSlots; ++m) {
+    const int i = lane + 32 * m;
+    cur[m] = i < n ? LLt[(size_t)(n - 1) * n + i] : 0.0;
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const int kn = k > 0 ? k - 1 : k;
 #pragma unroll
     for (int m = 0; m < kInvSlots; ++m) {
       const int i = lane + 32 * m;
-      if (i == k) y[m] = xk;
-      else if (i < k) y[m] = fma(-row[i], xk, y[m]);
+      nxt[m] = i < n ? LLt[(size_t)kn * n + i] : 0.0;
+    }
+    const int km = k >> 5;
+    double own = 0.0;
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m) own = m == km ? y[m] : own;
+    const double xk = __shfl_sync(0xffffffffu, own, k & 31) * idg[k];
+#pragma unroll
+    for (int m = 0; m < kInvSlots; ++m) {
+      const int i = lane + 32 * m;
+      const double upd = fma(-(i < k ? cur[m] : 0.0), xk, y[m]);
+      y[m] = i == k ? xk : upd;
+      cur[m] = nxt[m];
     }
   }
   const bool fj = (fix[j / 3] >> (j % 3)) & 1;
