@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(768) k_mgs_op(LevelView L, int R, const float*
 // each: these levels are small (a few thousand nodes) and latency-bound.
 // CTA: 32 consecutive nodes x kMgsRb right-hand sides x 3 components x 3
 // planes; grid.y covers the right-hand sides.
-constexpr int kMgsRb = 2;
+constexpr int kMgsRb = 1;
 __global__ void __launch_bounds__(32 * 9 * kMgsRb) k_mgs_op_split(LevelView L, int R, const float* __restrict__ x,
                                                                   const float* __restrict__ b, float* y,
                                                                   const float* __restrict__ coef, int mode) {
@@ -645,11 +645,11 @@ __global__ void __launch_bounds__(32 * 9 * kMgsRb) k_mgs_op_split(LevelView L, i
   if (q == 0) y[o + 3] = 0.f;
 }
 
-// The split form wins where the level is small for its R (measured on the
-// 2 mm arm: 3 136 nodes x 4 vectors 7.1 -> 4.8 us, 580 nodes x 8 vectors
-// 7.5 -> 4.2 us); at 3 136 nodes x 8 vectors the unsplit grid already has
-// enough threads (7.7 vs 8.1 us split).
-constexpr long long kMgsSplitBelow = 16384;   // nodes x right-hand sides
+// The split form wins on these small levels (measured on the 2 mm arm, one
+// right-hand side per CTA: 3 136 nodes x 4 vectors 7.1 -> 4.4 us, 3 136 x 8
+// 7.7 -> 7.1 us, 580 x 4 6.8 -> 3.8 us; with two right-hand sides per CTA
+// the 3 136 x 8 case was slower split, 8.1 us).
+constexpr long long kMgsSplitBelow = 32768;   // nodes x right-hand sides
 static void launch_mgs_op(const LevelView& L, int R, const float* x, const float* b, float* y, const float* coef,
                           int mode, cudaStream_t s) {
   if ((long long)L.NN * R <= kMgsSplitBelow)
