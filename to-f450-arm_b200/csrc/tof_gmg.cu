@@ -748,12 +748,14 @@ struct Transfer {
 // z-offsets: three threads of 9 loads, combined through shared memory in a
 // fixed order (the levels are small and the loads latency-bound; measured
 // on the 2 mm arm: V-cycle 100.7 -> 96.5 us with 4 vectors against one
-// thread of 27 loads).  CTA: 32 coarse nodes x 3 offsets x R.
-__global__ void __launch_bounds__(32 * 3 * TOF_MAX_RHS) k_mg_restrict_split(Transfer T, int R, const float* __restrict__ tf,
-                                                                          const uint8_t* __restrict__ fixc, float* rc) {
-  __shared__ float part[TOF_MAX_RHS][3][3][32];
+// thread of 27 loads).  CTA: 32 coarse nodes x 3 offsets of one
+// right-hand side (grid.y), so a small coarse level still spreads over many
+// SMs.
+__global__ void __launch_bounds__(32 * 3) k_mg_restrict_split(Transfer T, int R, const float* __restrict__ tf,
+                                                             const uint8_t* __restrict__ fixc, float* rc) {
+  __shared__ float part[3][3][32];
   const int NNc = T.NXc * T.NYc * T.NZc;
-  const int tx = threadIdx.x, c = threadIdx.y % 3, r = threadIdx.y / 3;
+  const int tx = threadIdx.x, c = threadIdx.y, r = blockIdx.y;
   const int N = blockIdx.x * 32 + tx;
   const bool live = N < NNc;
   const long long vsf = (long long)T.NXf * T.NYf * T.NZf * 4, vsc = (long long)NNc * 4;
@@ -776,14 +778,14 @@ __global__ void __launch_bounds__(32 * 3 * TOF_MAX_RHS) k_mg_restrict_split(Tran
       a0 = fmaf(w, v.x, a0); a1 = fmaf(w, v.y, a1); a2 = fmaf(w, v.z, a2);
     }
   }
-  part[r][c][0][tx] = a0;
-  part[r][c][1][tx] = a1;
-  part[r][c][2][tx] = a2;
+  part[c][0][tx] = a0;
+  part[c][1][tx] = a1;
+  part[c][2][tx] = a2;
   __syncthreads();
   if (!live || c != 0) return;
   float o[3];
 #pragma unroll
-  for (int q = 0; q < 3; ++q) o[q] = (part[r][0][q][tx] + part[r][1][q][tx]) + part[r][2][q][tx];
+  for (int q = 0; q < 3; ++q) o[q] = (part[0][q][tx] + part[1][q][tx]) + part[2][q][tx];
   const uint8_t fx = fixc[N];
   reinterpret_cast<float4*>(rc + r * vsc)[N] =
       make_float4((fx & 1) ? 0.f : o[0], (fx & 2) ? 0.f : o[1], (fx & 4) ? 0.f : o[2], 0.f);
@@ -1036,7 +1038,7 @@ static int vcycle_t(Ctx& c, int lane, cudaStream_t s) {
     if (k == 0) { if (launch_matvec(c, 0, false, cur[k], Bf[k].t, R, Bf[k].r, s)) return -2; }
     else launch_mgs_op(view(L), R, cur[k], Bf[k].r, Bf[k].t, nullptr, 0, s);
     MGLevel& C = mg->L[k + 1];
-    k_mg_restrict_split<<<ceil_div(C.NN, 32), dim3(32, 3 * R), 0, s>>>(transfer(L, C), R, Bf[k].t, C.fix,
+    k_mg_restrict_split<<<dim3(ceil_div(C.NN, 32), R), dim3(32, 3), 0, s>>>(transfer(L, C), R, Bf[k].t, C.fix,
                                                                        Bf[k + 1].r);
     count_launch();
   }
