@@ -204,8 +204,10 @@ int tof_mg_setup(tof_ctx* ctx, void* stream);
 
 /* Lowest `nmodes` eigenpairs of K_ff x = lam M_ff x with a block of `block`
  * vectors (nmodes <= block <= 8).  X (device node4 FP64, `block` vectors)
- * holds the start block on entry (warm start or random) and the
- * M-orthonormal modes, ascending, in its first nmodes vectors on exit;
+ * holds the start block on entry (warm start or random) and on exit the
+ * `block` M-orthonormal Ritz vectors of the final Rayleigh-Ritz step,
+ * ascending: the modes in its first nmodes vectors, then the guard vectors
+ * (a warm start for the next solve);
  * lam (host, nmodes) gets the eigenvalues (rad/s)^2.  Replaces
  * FEM3D.modal_analysis (src/fem.py:400-470) and _modal_gpu
  * (src/fem_gpu.py:101-173).  precond: TOF_PRECOND_JACOBI (as the reference),

@@ -844,7 +844,8 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   // (its Gram matrices go to slots 8 / 9)
   launch_gram2_cols(c, true, X6, KX6, MX6, ident, nb, c.gram + 8 * 576, c.gram + 9 * 576, s, c.gram_part_m);
   lob_small_eig(c, nb, nb, 1e-14, s, c.gram + 8 * 576, c.gram + 9 * 576);
-  // X64 = X6 C (first nmodes columns)
+  // X64 = X6 C: all nb Ritz vectors of the final step, the nmodes wanted
+  // ones first (the rest warm-start the guard columns of the next solve)
   {
     double* out = X64;
     // reuse the update kernel: S = X6 (ncols = nb), P part unused -> KS2/MS2 scratch
@@ -852,7 +853,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     if (f64) scratch = (double*)B.S[cur ^ 1];
     launch_lob_update<double>(NN, nb, nb, ident, vs, X6, KX6, MX6, C, scratch, scratch + 3LL * c.max_modes * vs,
                               scratch + 6LL * c.max_modes * vs, s);
-    cudaMemcpyAsync(out, scratch, sizeof(double) * nmodes * vs, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(out, scratch, sizeof(double) * nb * vs, cudaMemcpyDeviceToDevice, s);
     // rounding floor of each returned residual: eps ||(|K| + theta M)|x|||
     // / ||K x|| (M has no negative entries); the current-iterate buffers are
     // free by now

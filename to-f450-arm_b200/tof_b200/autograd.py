@@ -84,7 +84,7 @@ class SIMPObjective:
             raise L.SolverError("tof_lobpcg", st["status"],
                                 f"modal solve stopped at residual {st['relres']:.2e} (tolerance {self.modal_tol:.1e})")
         self.modal_stats = st
-        self.X4 = torch.cat([modes, self.X4[n:]]) if nb > n else modes.clone()
+        self.X4 = ctx.last_block                        # all final Ritz vectors: the next warm start
         return modes, np.maximum(lam, 0.0)
 
     def evaluate(self, x: torch.Tensor) -> dict:

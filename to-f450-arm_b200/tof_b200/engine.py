@@ -140,7 +140,9 @@ class DesignContext:
     def lobpcg(self, X4: torch.Tensor, nmodes: int, tol=1e-5, maxiter=500, mode=L.MODE_MIXED,
                precond=L.PRECOND_PCG, inner_iters=60, inner_rtol=1e-2, raise_on_error=True, mg_cycles=1):
         """Lowest nmodes of K x = lam M x from the start block X4 (block, NN, 4).
-        mg_cycles: V-cycles per preconditioner application (multigrid)."""
+        mg_cycles: V-cycles per preconditioner application (multigrid).
+        Returns the modes (the first nmodes Ritz vectors); all `block` Ritz
+        vectors of the final step are kept in self.last_block."""
         if precond == L.PRECOND_MG or mode == L.MODE_MIXED:
             inner_iters = mg_cycles
         X = X4.to(torch.float64).contiguous().clone()
@@ -153,6 +155,7 @@ class DesignContext:
         stats = dict(status=st.status, iters=st.iters, relres=st.relres, floor=st.floor, resid=list(res))
         self.last_stats = [stats]
         self.last_rc = rc
+        self.last_block = X
         if raise_on_error:
             L.check("tof_lobpcg", rc, self.h, allow=(L.TOF_OK, L.TOF_NOT_CONVERGED))
         return X[:nmodes], np.array(list(lam)), stats

@@ -215,8 +215,8 @@ class SIMPOptimizer:
         modes, lam, st = ctx.lobpcg(X4, n, tol=self.modal_tol, maxiter=maxit, mode=mid,
                                     precond=L.PRECOND_MG if mid == L.MODE_MIXED else L.PRECOND_JACOBI,
                                     mg_cycles=self.modal_mg_cycles)
-        # warm start: converged modes plus the previous guard vectors
-        self.X4 = torch.cat([modes, X4[n:]]) if nb > n else modes.clone()
+        # warm start: the final Ritz vectors, modes and guard vectors
+        self.X4 = ctx.last_block
         self.stats.append(("lobpcg", st))
         self.history["modal_converged"].append(st["status"] == L.TOF_OK)
         self.history["modal_iters"].append(st["iters"])
