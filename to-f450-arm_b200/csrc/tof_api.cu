@@ -493,6 +493,30 @@ static int true_relres(Ctx& c, const double* b, const double* x, int R, double* 
   return TOF_OK;
 }
 
+// Status of one right-hand side after a PCG pass, given its true relative
+// residual `rel` and the target max(rtol, rounding floor); sets `again`
+// when the pass should be followed by a restart from the current x.  A
+// pass that claims convergence above the target restarts (residual
+// replacement).  So does a CG breakdown (p^T K p <= 0 in floating point):
+// near the rounding floor the search direction is rounding noise and its
+// energy can come out non-positive, and a restart recomputes the residual
+// and the direction in FP64.  A breakdown at the target is convergence; one
+// in the last allowed pass ends the solve not converged (the current x is
+// the best one).
+static int settle_pass(int status, double rel, double target, bool last, bool& again) {
+  if (status == ST_BREAKDOWN) {
+    if (rel <= target * 1.01) return ST_OK;
+    if (last) return ST_NOT_CONVERGED;
+    again = true;
+    return ST_NOT_CONVERGED;
+  }
+  if (status == ST_OK && rel > target * 1.01) {
+    again = true;
+    return ST_NOT_CONVERGED;
+  }
+  return status;
+}
+
 int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double rtol, int maxiter,
             tof_solve_stats* stats, void* stream) {
   if (!ctx || !b || !x || nrhs < 1 || !(rtol > 0.0) || maxiter < 1) return TOF_ERR_ARG;
@@ -532,8 +556,7 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       for (int k = 0; k < nrhs; ++k) {
         iters[k] += sto[R + k];
         outer[k] = o + 1;
-        st[k] = sto[k];
-        if (st[k] == ST_OK && rel[k] > std::max(rtol, phi[k]) * 1.01) { st[k] = ST_NOT_CONVERGED; again = true; }
+        st[k] = settle_pass(sto[k], rel[k], std::max(rtol, phi[k]), o == kMaxRestarts, again);
       }
       if (!again) break;
     }
@@ -555,8 +578,7 @@ int tof_pcg(tof_ctx* ctx, int mode, const double* b, double* x, int nrhs, double
       for (int k = 0; k < nrhs; ++k) {
         iters[k] += it_o[k];
         outer[k] = o + 1;
-        st[k] = ist[k];
-        if (st[k] == ST_OK && rel[k] > std::max(rtol, phi[k]) * 1.01) { st[k] = ST_NOT_CONVERGED; again = true; }
+        st[k] = settle_pass(ist[k], rel[k], std::max(rtol, phi[k]), o == kMaxRestarts, again);
       }
       if (!again) break;
     }
