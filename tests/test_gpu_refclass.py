@@ -1,7 +1,8 @@
 """The drop-in on the reference's own classes.
 
 `enable_b200_solver` is applied to the reference's `src.fem.FEM3D` and
-`src.topopt` (the reference installed in baseline/_ref) and
+`src.topopt` (the reference package installed into baseline/_ref with pip's
+`--target`) and
 the reference's own code runs on top of it:
 
 * its `SIMPOptimizer.run` (src/topopt.py:217-427) for four iterations of the
@@ -35,7 +36,7 @@ REF = os.path.join(ROOT, "baseline", "_ref")
 @pytest.fixture(scope="module")
 def ref():
     if not os.path.isfile(os.path.join(REF, "src", "fem.py")):
-        pytest.fail("the reference is not installed in baseline/_ref (DESIGN.md: reference install)")
+        pytest.fail("the reference is not installed in baseline/_ref (pip install --target baseline/_ref <checkout>)")
     if REF not in sys.path:
         sys.path.insert(0, REF)
     import src.fem as rfem
