@@ -94,6 +94,7 @@ def test_quadform_compliance(tiny):
 
 @pytest.mark.parametrize("mode", [0, 1])
 def test_lobpcg_tiny(tiny, mode):
+    from tof_b200 import _lib as L
     g, ctx = tiny
     rng = np.random.default_rng(0)
     X0 = ctx.pack(to_dev(rng.standard_normal((6, 3 * ctx.NN))))
@@ -102,6 +103,16 @@ def test_lobpcg_tiny(tiny, mode):
     assert rel(freqs, g["freqs"]) < 1e-7, (freqs, g["freqs"], st)
     eff = ctx.effective_mass(X)
     assert np.max(np.abs(eff - g["eff"])) < 1e-6
+    # all block Ritz vectors come back (the warm start of the next solve):
+    # M-orthonormal, Rayleigh quotients ascending, the first four the modes
+    B = ctx.last_block
+    assert B.shape[0] == 6 and torch.equal(B[:4], X)
+    GM = ctx.gram(B, ctx.matvec(L.OP_M, B)).cpu().numpy()
+    GK = ctx.gram(B, ctx.matvec(L.OP_K, B)).cpu().numpy()
+    assert np.max(np.abs(GM - np.eye(6))) < 1e-8
+    rq = np.diag(GK) / np.diag(GM)
+    assert np.all(np.diff(rq) >= -1e-8 * rq[-1])
+    assert rel(rq[:4], lam) < 1e-8
 
 
 def test_filter_and_oc(golden):
