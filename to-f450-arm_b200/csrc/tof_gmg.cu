@@ -97,16 +97,22 @@ struct MG {
   double* part = nullptr;     // partial sums
   int part_blocks = 0;
   int* info = nullptr;
-  // captured PCG iterations (kGraphIters per graph), one per R = 1, 2, 4, 8
-  cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
-  size_t gnodes[4] = {0, 0, 0, 0};
-  bool graph_failed = false;
-  // a single V-cycle per lane and R, replayed by callers outside the PCG graphs
+  // a single V-cycle per lane and R, replayed by every caller
   cudaGraphExec_t vexec[kLanes][4] = {};
   size_t vnodes[kLanes][4] = {};
   bool vgraph_failed = false;
 };
-constexpr int kGraphIters = 4;   // even: p double-buffer parity returns to 0
+// MG-PCG iterations between host checks of the convergence flags (even:
+// the p double-buffer parity returns to 0), launched kernel by kernel (the
+// V-cycle inside each is a graph replay).  This paces the static solve: in
+// the SIMP step it runs beside the modal solve, whose chain of short kernels
+// is the critical path, and a static stream that never pauses slows that
+// chain down.  Measured on the 2 mm arm, per design iteration in the timed
+// window: groups of 8 / 4 / 2 iterations replayed as graphs 78 / 73 / 63 ms,
+// launched kernel by kernel 61 ms (4) and 59 ms (2); a device-side loop
+// without host checks was slower still.  A standalone 4-vector solve costs
+// ~5 % more than with graph groups (30.4 vs 28.8 ms).
+constexpr int kCheckIters = 2;
 
 // ---------------------------------------------------------------------------
 // small helpers
@@ -938,8 +944,6 @@ void mg_destroy(Ctx& c) {
       cudaFree(B.r); cudaFree(B.e); cudaFree(B.e2); cudaFree(B.t);
     }
   }
-  for (auto& g : mg->gexec)
-    if (g) cudaGraphExecDestroy(g);
   for (auto& lane : mg->vexec)
     for (auto& g : lane)
       if (g) cudaGraphExecDestroy(g);
@@ -1117,7 +1121,7 @@ int mg_capture_all(Ctx& c) {
 }
 
 // Apply the V-cycle to mg_rhs(c, lane) (R vectors); result in mg_out(c, lane).
-// Inside a stream capture (the PCG graphs) the kernels are recorded as they
+// Inside a stream capture (tof_time_kernel's graphs) the kernels are recorded as they
 // are; otherwise the recorded graph of this lane and R is replayed, which
 // removes the per-kernel launch overhead of ~40 short launches.
 int mg_vcycle(Ctx& c, int R, cudaStream_t s, int lane) {
@@ -1431,41 +1435,17 @@ static int mgpcg_t(Ctx& c, const double* b, double* x, double rtol, int maxiter,
   count_launch();
   int it = 0;
   int hf[9];
-  const int ri = R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : 3;
   while (true) {
     cudaMemcpyAsync(hf, mg->flags, sizeof(int) * 9, cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) { c.last_error = "multigrid PCG: CUDA error"; return -2; }
     bool all = true;
     for (int k = 0; k < R; ++k) all = all && hf[k] != 0;
     if (all || it >= maxiter || hf[8]) break;
-    // kGraphIters iterations per step: a replay of the captured graph when
-    // the stream can be captured, else eager launches (same kernels)
-    if (!mg->gexec[ri] && !mg->graph_failed) {
-      cudaGraph_t graph = nullptr;
-      bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-      capturing() = ok;
-      for (int q = 0; ok && q < kGraphIters; ++q) ok = mgpcg_iter<R>(c, q & 1, s) == 0;
-      capturing() = false;
-      const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
-      if (ok && ended && graph && cudaGraphInstantiate(&mg->gexec[ri], graph, 0) == cudaSuccess) {
-        cudaGraphGetNodes(graph, nullptr, &mg->gnodes[ri]);
-      } else {
-        mg->gexec[ri] = nullptr;
-        mg->graph_failed = true;
-      }
-      if (graph) cudaGraphDestroy(graph);
-      cudaGetLastError();   // clear a refused capture (e.g. the legacy default stream)
-    }
-    // never more than maxiter iterations: a remainder shorter than the
-    // captured group runs eagerly
-    const int step = std::min(kGraphIters, maxiter - it);
-    if (mg->gexec[ri] && step == kGraphIters) {
-      if (cudaGraphLaunch(mg->gexec[ri], s) != cudaSuccess) { c.last_error = "multigrid PCG: graph launch"; return -2; }
-      count_launch((long long)mg->gnodes[ri]);
-    } else {
-      for (int q = 0; q < step; ++q)
-        if (mgpcg_iter<R>(c, q & 1, s)) return -2;
-    }
+    // kCheckIters iterations between two host checks of the flags, each
+    // kernel launched on its own (never more than maxiter iterations)
+    const int step = std::min(kCheckIters, maxiter - it);
+    for (int q = 0; q < step; ++q)
+      if (mgpcg_iter<R>(c, q & 1, s)) return -2;
     it += step;
   }
   cudaMemcpyAsync(x, mg->x, sizeof(double) * R * V, cudaMemcpyDeviceToDevice, s);
