@@ -30,7 +30,7 @@ namespace tof {
 
 constexpr int kMaxBasis = 24;
 #ifndef TOF_LOB_REFRESH
-#define TOF_LOB_REFRESH 10
+#define TOF_LOB_REFRESH 20
 #endif
 constexpr int kLobRefresh = TOF_LOB_REFRESH;   // iterations between fresh K / M products
 // Below its rounding floor (~eps * lambda_max / lambda_1 of the pencil) the
