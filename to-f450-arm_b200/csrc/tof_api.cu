@@ -121,6 +121,9 @@ static void free_ctx(Ctx& c) {
   mg_destroy(c);
   for (cudaEvent_t& e : c.lob_ev)
     if (e) { cudaEventDestroy(e); e = nullptr; }
+  if (c.lob_cev) { cudaEventDestroy(c.lob_cev); c.lob_cev = nullptr; }
+  if (c.lob_pev) { cudaEventDestroy(c.lob_pev); c.lob_pev = nullptr; }
+  if (c.lob_side) { cudaStreamDestroy(c.lob_side); c.lob_side = nullptr; }
   if (c.lob_pin) { cudaFreeHost(c.lob_pin); c.lob_pin = nullptr; }
   void* ptrs[] = {c.Ke64, c.Me64, c.keb64, c.meb64, c.kebabs64, c.keb32, c.meb32, c.active, c.fix, c.tip64, c.tip32,
                   c.fK64, c.fM64, c.fK32, c.fM32, c.rho, c.dK64, c.dM64, c.dinvK64, c.dinvK32, c.partials,
@@ -289,6 +292,9 @@ int tof_ctx_create(int nx, int ny, int nz, const double h[3], const double Ke[57
   A(cudaHostAlloc(&c.lob_pin, 3 * 256, cudaHostAllocMapped));
   if (c.lob_pin) A(cudaHostGetDevicePointer(&c.lob_pin_dev, c.lob_pin, 0));
   for (cudaEvent_t& ev : c.lob_ev) A(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&c.lob_cev, cudaEventDisableTiming));
+  A(cudaEventCreateWithFlags(&c.lob_pev, cudaEventDisableTiming));
+  A(cudaStreamCreateWithFlags(&c.lob_side, cudaStreamNonBlocking));
   if (e != cudaSuccess) return fail(std::string("tof_ctx_create: ") + cudaGetErrorString(e));
   if (mg_create(c, c.max_rhs)) return fail("tof_ctx_create: " + c.last_error.str());
   mg_capture_all(c);

@@ -129,6 +129,10 @@ struct Ctx {
   // the events that mark them complete
   void* lob_pin = nullptr;       // 3 slots of 256 bytes (cudaHostAlloc, mapped)
   void* lob_pin_dev = nullptr;
+  // LOBPCG: a side stream for the P half of the block update (off the
+  // critical path) and the events that order it: C ready, P half done
+  cudaStream_t lob_side = nullptr;
+  cudaEvent_t lob_cev = nullptr, lob_pev = nullptr;
   cudaEvent_t lob_ev[3] = {nullptr, nullptr, nullptr};
 
   // persistent-launch capacity for each kernel flavour

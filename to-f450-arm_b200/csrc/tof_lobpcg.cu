@@ -469,16 +469,17 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, ColMap cols, long long vs,
                                                     const T* __restrict__ S, const T* __restrict__ KS,
                                                     const T* __restrict__ MS, const double* __restrict__ C,
-                                                    T* S2, T* KS2, T* MS2) {
+                                                    T* S2, T* KS2, T* MS2, int only) {
   using V4 = typename Vec4<T>::type;
   __shared__ T sC[kMaxBasis * 8];
   for (int i = threadIdx.x; i < ncols * nb; i += blockDim.x) sC[i] = T(C[i]);
   __syncthreads();
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= 6LL * NN) return;
+  if (t >= (only >= 0 ? 3LL : 6LL) * NN) return;
   const int n = int(t % NN);
   const int b = int((t / NN) % 3);
-  const int half = int(t / (3LL * NN));      // 0: X = S C, 1: P = S[:, nb:] C[nb:, :]
+  // 0: X = S C, 1: P = S[:, nb:] C[nb:, :] (`only` >= 0: that half alone)
+  const int half = only >= 0 ? only : int(t / (3LL * NN));
   const T* src = b == 0 ? S : b == 1 ? KS : MS;
   T* dst = b == 0 ? S2 : b == 1 ? KS2 : MS2;
   const int j0 = half ? nb : 0;
@@ -513,8 +514,10 @@ __global__ void __launch_bounds__(128) k_lob_update(int NN, int nb, int ncols, C
 
 template <typename T>
 static void launch_lob_update(int NN, int nb, int ncols, const ColMap& cols, long long vs, const T* S, const T* KS,
-                              const T* MS, const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s) {
-  k_lob_update<T><<<int((6LL * NN + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2);
+                              const T* MS, const double* C, T* S2, T* KS2, T* MS2, cudaStream_t s, int only = -1) {
+  const long long threads = (only >= 0 ? 3LL : 6LL) * NN;
+  k_lob_update<T><<<int((threads + 127) / 128), 128, 0, s>>>(NN, nb, ncols, cols, vs, S, KS, MS, C, S2, KS2, MS2,
+                                                             only);
   count_launch();
 }
 
@@ -581,6 +584,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   const int rblocks = 2 * c.num_sms;
   int cur = 0;
   if (precond == 2 && mg_ensure(c, s)) return -2;
+  cudaStreamWaitEvent(s, c.lob_pev, 0);        // a P half still running from an earlier call
   // X <- X64 (first nb vectors), KX, MX
   launch_convert(X64, true, B.S[cur], f64, (long long)nb * vs, s);
   if (launch_matvec_km(c, f64, B.S[cur], B.KS[cur], B.MS[cur], nb, s)) return -2;
@@ -606,6 +610,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
   // wanted residuals; recomputing the products every kLobRefresh iterations
   // (and before convergence is accepted) bounds that drift.
   auto refresh = [&]() -> int {
+    cudaStreamWaitEvent(s, c.lob_pev, 0);      // P of this iterate (side stream)
     void* S = B.S[cur];
     if (launch_matvec_km(c, f64, S, B.KS[cur], B.MS[cur], nb, s)) return -2;
     const T* P = vec<T>(S, 2 * nb, vs);
@@ -811,6 +816,7 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
     for (int k = ncols; k < 24; ++k) cols.col[k] = 0;
     drop_p = false;
     ncols_at[it & 1] = ncols;
+    cudaStreamWaitEvent(s, c.lob_pev, 0);      // P, K P, M P of this iterate
     launch_gram2_cols(c, f64, B.S[cur], B.KS[cur], B.MS[cur], cols, ncols, GK, GM, s, c.gram_part_m);
     // keep a full-basis problem for tof_time_kernel: the first one, then
     // one every 16 iterations (a 9 KB copy), so it comes from the late,
@@ -821,10 +827,18 @@ static int lobpcg_impl(Ctx& c, int nmodes, int nb, double* X64, double* lam, dou
       c.lob_last_m = nb;
     }
     lob_small_eig(c, ncols, nb, drop, s);
+    // the P half of the update on the side stream: the next iteration needs
+    // only X, K X, M X until its Gram matrices (which wait for it)
+    cudaEventRecord(c.lob_cev, s);
+    cudaStreamWaitEvent(c.lob_side, c.lob_cev, 0);
     launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
-                         (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s);
+                         (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], c.lob_side, 1);
+    cudaEventRecord(c.lob_pev, c.lob_side);
+    launch_lob_update<T>(NN, nb, ncols, cols, vs, (T*)B.S[cur], (T*)B.KS[cur], (T*)B.MS[cur], C,
+                         (T*)B.S[cur ^ 1], (T*)B.KS[cur ^ 1], (T*)B.MS[cur ^ 1], s, 0);
     cur ^= 1;
   }
+  cudaStreamWaitEvent(s, c.lob_pev, 0);        // the last P half, before anything reads the buffers
   if (pending >= 0 && !conv && !use_best) {    // the last iterate's residual, not yet read
     if (read_resid(pending)) return -2;
     ncols_prev = it >= 2 ? ncols_at[(it - 2) & 1] : nb;
